@@ -1,0 +1,109 @@
+"""Run the compiled reference projection (oracle/_ref) on a scene.
+
+Test infrastructure only: the product never imports this module. It writes a
+scene with ``Scene.write_reference_input``, runs ``shkz_ref_harness`` from
+``oracle/_ref/<variant>/`` (built by ``oracle/ref/Makefile`` from the
+reference's own sources) and reads back what the reference grids hold after
+``macpressuresolver3::project`` (src/projection/macpressuresolver3.cpp:54-299).
+"""
+from __future__ import annotations
+
+import dataclasses
+import os
+import struct
+import subprocess
+import tempfile
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+
+
+def ref_available(variant: str = "float") -> bool:
+    return os.path.exists(os.path.join(REF_DIR, variant, "shkz_ref_harness"))
+
+
+@dataclasses.dataclass
+class RefResult:
+    fluid: np.ndarray
+    fluid_active: np.ndarray
+    solid: np.ndarray
+    solid_active: np.ndarray
+    velocity_in: list
+    velocity_in_active: list
+    pressure: np.ndarray
+    pressure_active: np.ndarray
+    velocity: list
+    velocity_active: list
+    projection_ms: float
+    iterations: Optional[int] = None
+    reresid: Optional[float] = None
+    solve_ms: Optional[float] = None
+    system: Optional[dict] = None
+
+
+def _read_cells(f, shape_zyx):
+    n = int(np.prod(shape_zyx))
+    v = np.frombuffer(f.read(8 * n), dtype=np.float64).reshape(shape_zyx)
+    m = np.frombuffer(f.read(n), dtype=np.uint8).reshape(shape_zyx)
+    return v, m
+
+
+def read_system(path: str) -> dict:
+    with open(path, "rb") as f:
+        n, nnz = struct.unpack("<2Q", f.read(16))
+        indptr = np.frombuffer(f.read(8 * (n + 1)), dtype=np.uint64).astype(np.int64)
+        indices = np.frombuffer(f.read(8 * nnz), dtype=np.uint64).astype(np.int64)
+        data = np.frombuffer(f.read(8 * nnz), dtype=np.float64)
+        rhs = np.frombuffer(f.read(8 * n), dtype=np.float64)
+    return {"n": n, "indptr": indptr, "indices": indices, "data": data, "rhs": rhs}
+
+
+def run_reference(scene, variant: str = "float", mode: str = "mic0", tol: Optional[float] = None,
+                  threads: Optional[int] = None, tile_size: int = 8, dump_system: bool = True,
+                  repeat: int = 1, extra: Optional[dict] = None, linsolver: str = "refmic0") -> RefResult:
+    exe = os.path.join(REF_DIR, variant, "shkz_ref_harness")
+    if not os.path.exists(exe):
+        raise FileNotFoundError(exe)
+    nx, ny, nz = scene.nx, scene.ny, scene.nz
+    with tempfile.TemporaryDirectory() as td:
+        inp = os.path.join(td, "in.bin")
+        out = os.path.join(td, "out.bin")
+        scene.write_reference_input(inp)
+        args = [exe, inp, out, f"LinSolver={linsolver}", f"RefMode={mode}",
+                f"Residual={tol if tol is not None else scene.tol}", f"TileSize={tile_size}",
+                f"Threads={threads or os.cpu_count()}", f"HarnessRepeat={repeat}"]
+        for k, v in (extra or {}).items():
+            args.append(f"{k}={v}")
+        env = dict(os.environ)
+        env["LD_LIBRARY_PATH"] = os.path.join(REF_DIR, variant) + ":" + env.get("LD_LIBRARY_PATH", "")
+        dump = os.path.join(td, "dump")
+        env["SHKZ_REF_DUMP"] = dump if dump_system else ""
+        proc = subprocess.run(args, cwd=td, env=env, capture_output=True, text=True)
+        if proc.returncode != 0:
+            raise RuntimeError(f"reference harness failed ({proc.returncode}):\n{proc.stdout[-3000:]}\n{proc.stderr[-3000:]}")
+        with open(out, "rb") as f:
+            assert f.read(8) == b"SHKZOUT1"
+            hx, hy, hz, real_bytes = struct.unpack("<4i", f.read(16))
+            cs = (nz, ny, nx)
+            ns = (nz + 1, ny + 1, nx + 1)
+            fs = [(nz, ny, nx + 1), (nz, ny + 1, nx), (nz + 1, ny, nx)]
+            fluid, fluid_m = _read_cells(f, cs)
+            solid, solid_m = _read_cells(f, ns)
+            vin = [_read_cells(f, s) for s in fs]
+            p, pm = _read_cells(f, cs)
+            vout = [_read_cells(f, s) for s in fs]
+            ms = struct.unpack("<d", f.read(8))[0]
+        res = RefResult(fluid=fluid, fluid_active=fluid_m, solid=solid, solid_active=solid_m,
+                        velocity_in=[v for v, _ in vin], velocity_in_active=[m for _, m in vin],
+                        pressure=p, pressure_active=pm,
+                        velocity=[v for v, _ in vout], velocity_active=[m for _, m in vout],
+                        projection_ms=ms)
+        if dump_system and os.path.exists(dump + ".solve.txt"):
+            it, rr, sms = open(dump + ".solve.txt").read().split()
+            res.iterations, res.reresid, res.solve_ms = int(it), float(rr), float(sms)
+        if dump_system and os.path.exists(dump + ".system.bin"):
+            res.system = read_system(dump + ".system.bin")
+        return res
