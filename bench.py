@@ -1,0 +1,396 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 pressure projection.
+
+Metric: ms per projection (and PCG iterations) to 1e-6 relative residual
+(infinity norm, the reference's stopping rule) on the 256^3 sloshing-tank
+workload: free surface y = 0.5 + 0.1 sin(2 pi x) cos(2 pi z), eight seeded
+solid boxes, Gaussian face velocities (sigma 0.5), dt = 0.005.
+
+A step is one full projection (labelling, tile pool, weights/rhs, MIC(0)
+factor, FP32 PCG with FP64 reductions and refinement, velocity update), on
+inputs already resident in HBM, preceded by a device copy that restores the
+input velocity (the projection updates it in place). ``e2e`` is the same
+projection through the host-buffer C-ABI call with pinned host arrays, so the
+host-device copies are inside its timed region.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Multi-GPU runs are independent replicas (the projection does not shard):
+each rank projects its own copy; the time is the maximum over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "ms/projection & PCG iters to 1e-6 rel. residual at 256³: learned vs plain, 1 B200"
+UNIT = "ms/projection"
+
+# Algorithmic bytes per pool cell (cells of 8^3 tiles holding >= 1 unknown)
+# for each kernel, FP32 data: reads + writes of the arrays it must touch once.
+ALGO_BYTES = {
+    "spmv": 24,        # x 4 + diag 4 + 3 lower weights 12 + y 4
+    "mic_sweeps": 52,  # forward: r, d, 3 w, write t (24); backward: t, d, 3 w, r, write z (28)
+    "update_xr": 24,   # read p, q, x, r; write x, r
+    "update_p": 12,    # read z, p; write p
+}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """Per-launch DRAM bytes of the stencil kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    if os.path.exists(p):
+        try:
+            return json.load(open(p))
+        except Exception:
+            return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sms, maxes, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sms.append(float(parts[1]))
+                maxes.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() in ("active", "1"):
+                    reasons.add(nm)
+        if not sms:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sms), "sm_max_mhz": max(maxes), "reasons": sorted(reasons),
+                "samples": len(sms)}
+
+
+def cpu_reference_sample(n: int = 128):
+    """The compiled reference (oracle/_ref) on a bounded sample of the workload:
+    the same scene at n^3, timed with the reference's own projection path."""
+    from shiokaze_b200 import scenes
+    from oracle import ref_runner
+    sc = scenes.sloshing_tank(n=n, seed=0, tol=1e-6)
+    if ref_runner.ref_available("float"):
+        r = ref_runner.run_reference(sc, mode="mic0", dump_system=True)
+        return {"value": r.projection_ms, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                "sample": f"sloshing tank {n}^3 (1/{(256 // n) ** 3} of the 256^3 cells), reference "
+                          f"macpressuresolver3 + MIC(0)-PCG to 1e-6, Threads={os.cpu_count()} (its PCG is "
+                          f"single-threaded), {r.iterations} iterations, 1 projection"}
+    from oracle import oracle
+    t = time.perf_counter()
+    o = oracle.project(sc, mic0=True)
+    ms = (time.perf_counter() - t) * 1e3
+    return {"value": ms, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"sloshing tank {n}^3, C restatement of the reference, MIC(0)-PCG to 1e-6, "
+                      f"{o.iterations} iterations, 1 projection"}
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from shiokaze_b200 import scenes
+    from oracle import ref_runner
+    n = args.n
+    sc = scenes.sloshing_tank(n=n, seed=0, tol=1e-6)
+    budget_s = float(os.environ.get("SHKZ_REF_BUDGET_S", "240"))
+    times, iters = [], None
+    kind = "reference" if ref_runner.ref_available("float") else "port"
+    t_start = time.perf_counter()
+    while len(times) < max(1, args.steps):
+        if kind == "reference":
+            r = ref_runner.run_reference(sc, mode="mic0", dump_system=True)
+            times.append(r.projection_ms)
+            iters = r.iterations
+        else:
+            from oracle import oracle
+            t = time.perf_counter()
+            o = oracle.project(sc, mic0=True)
+            times.append((time.perf_counter() - t) * 1e3)
+            iters = o.iterations
+        if time.perf_counter() - t_start > budget_s:
+            break
+    value = float(np.mean(times))
+    cores = os.cpu_count() if kind == "reference" else 1
+    sample = (f"sloshing tank {n}^3, reference macpressuresolver3 with MIC(0)-PCG to 1e-6 "
+              f"({iters} iterations), {len(times)} of {args.steps} requested projections within a "
+              f"{budget_s:.0f} s budget, no warm-up (CPU path has no warm state)")
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": len(times),
+            "warmup": 0, "ms_per_step": value, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 system, f32 grids", "data": "synthetic",
+            "impl": "reference", "iterations": iters,
+            "config": {"workload": f"sloshing_tank {n}^3, plain MIC(0)-PCG projection to 1e-6 (inf-norm)",
+                       "seed": 0},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--precond", default="mic0", choices=["mic0", "none", "learned"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    args.warmup = max(args.warmup, 3)
+
+    import torch
+    import torch.distributed as dist
+    from shiokaze_b200 import native, scenes
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    sc = scenes.sloshing_tank(n=args.n, seed=0, tol=1e-6)
+    nx, ny, nz = sc.nx, sc.ny, sc.nz
+
+    cfg = native.default_config()
+    cfg.residual = 1e-6
+    cfg.preconditioner = {"mic0": native.PRECOND_MIC0, "none": native.PRECOND_NONE,
+                          "learned": native.PRECOND_LEARNED}[args.precond]
+    cfg.device = local
+    ctx = native.Context(cfg)
+    L = native.load()
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+
+    # device-resident inputs
+    def dev_t(a, dtype):
+        return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    fluid = dev_t(sc.fluid_effective(), np.float32)
+    fact = dev_t(sc.fluid_active.astype(np.uint8), np.uint8)
+    solid = dev_t(sc.solid_effective(), np.float32)
+    sact = dev_t(sc.solid_active.astype(np.uint8), np.uint8)
+    vel0 = [dev_t(v, np.float32) for v in sc.velocity_effective()]
+    vact0 = [dev_t(m.astype(np.uint8), np.uint8) for m in sc.velocity_active]
+    vel = [v.clone() for v in vel0]
+    vact = [m.clone() for m in vact0]
+    pressure = torch.zeros((nz, ny, nx), dtype=torch.float32, device=dev)
+    pact = torch.zeros((nz, ny, nx), dtype=torch.uint8, device=dev)
+    torch.cuda.synchronize(dev)
+
+    a = native.ProjectArgs()
+    a.nx, a.ny, a.nz, a.dx, a.dt = nx, ny, nz, sc.dx, sc.dt
+    a.fluid, a.fluid_active = fluid.data_ptr(), fact.data_ptr()
+    a.solid, a.solid_active = solid.data_ptr(), sact.data_ptr()
+    for d in range(3):
+        a.velocity[d] = vel[d].data_ptr()
+        a.velocity_active[d] = vact[d].data_ptr()
+        a.solid_velocity[d] = None
+    a.pressure, a.pressure_active = pressure.data_ptr(), pact.data_ptr()
+    res = native.Result()
+
+    def step():
+        with torch.cuda.stream(stream):
+            for d in range(3):
+                vel[d].copy_(vel0[d], non_blocking=True)
+                vact[d].copy_(vact0[d], non_blocking=True)
+        rc = L.shkz_b200_project_device(ctx.handle, ctypes.byref(a), ctypes.byref(res))
+        if rc != 0:
+            raise native.ShkzError(rc, "shkz_b200_project_device", ctx.last_error())
+        return res.as_dict()
+
+    for _ in range(args.warmup):
+        step()
+    results = []
+    launches = 0
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            r = step()
+            results.append(r)
+            launches += r["kernel_launches"]  # the restore copies are torch copies, not counted
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    elapsed_ms = ev0.elapsed_time(ev1)
+    t = torch.tensor([elapsed_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    elapsed_ms = float(t.item())
+    total_proj = args.steps * world
+    value = elapsed_ms / total_proj if world > 1 else elapsed_ms / args.steps
+    clocks = clk.summary()
+    last = results[-1]
+
+    # kernel timings on the last system (CUDA events on the context stream)
+    kern = {}
+    ms = ctypes.c_double()
+    cells = ctypes.c_longlong()
+    for name, which in (("spmv", 0), ("mic_sweeps", 1), ("update_xr", 3), ("update_p", 4),
+                        ("label", 5), ("coeff", 6), ("mic_factor", 7)):
+        rc = L.shkz_b200_time_kernel(ctx.handle, which, 30 if which != 7 else 5, ctypes.byref(ms), ctypes.byref(cells))
+        if rc != 0:
+            kern[name] = {"error": rc}
+            continue
+        entry = {"ms": ms.value, "cells": cells.value}
+        if name in ALGO_BYTES:
+            gbs = ALGO_BYTES[name] * cells.value / (ms.value * 1e-3) / 1e9
+            entry["algo_bytes_per_cell"] = ALGO_BYTES[name]
+            entry["achieved_gbs"] = gbs
+        kern[name] = entry
+    peak, peak_kind = measured_peaks()
+    sp = kern.get("spmv", {})
+    traffic = ncu_traffic()
+    traffic_bytes = None
+    if traffic and "spmv" in traffic and sp.get("cells"):
+        t0 = traffic["spmv"]
+        traffic_bytes = t0["dram_bytes_per_launch"] * sp["cells"] / t0["cells"]
+    roofline = None
+    if "achieved_gbs" in sp:
+        roofline = {"kernel": "k_spmv (7-point stencil q = A p with fused p.q)", "bound": "hbm",
+                    "achieved": sp["achieved_gbs"], "peak": peak, "unit": "GB/s",
+                    "frac": sp["achieved_gbs"] / peak, "peak_kind": peak_kind,
+                    "algo_bytes_per_launch": ALGO_BYTES["spmv"] * sp["cells"],
+                    "traffic": traffic_bytes}
+
+    # end to end through the host-buffer C-ABI call with pinned host memory
+    e2e = None
+    if rank == 0 or world > 1:
+        pin = lambda arr: torch.from_numpy(np.ascontiguousarray(arr)).pin_memory()
+        h_fluid, h_fact = pin(sc.fluid_effective()), pin(sc.fluid_active.astype(np.uint8))
+        h_solid, h_sact = pin(sc.solid_effective()), pin(sc.solid_active.astype(np.uint8))
+        h_vel0 = [v.copy() for v in sc.velocity_effective()]
+        h_vact0 = [m.astype(np.uint8).copy() for m in sc.velocity_active]
+        h_vel = [pin(v) for v in h_vel0]
+        h_vact = [pin(m) for m in h_vact0]
+        h_p = torch.zeros((nz, ny, nx), dtype=torch.float32).pin_memory()
+        h_pa = torch.zeros((nz, ny, nx), dtype=torch.uint8).pin_memory()
+        ha = native.ProjectArgs()
+        ha.nx, ha.ny, ha.nz, ha.dx, ha.dt = nx, ny, nz, sc.dx, sc.dt
+        ha.fluid, ha.fluid_active = h_fluid.data_ptr(), h_fact.data_ptr()
+        ha.solid, ha.solid_active = h_solid.data_ptr(), h_sact.data_ptr()
+        for d in range(3):
+            ha.velocity[d] = h_vel[d].data_ptr()
+            ha.velocity_active[d] = h_vact[d].data_ptr()
+            ha.solid_velocity[d] = None
+        ha.pressure, ha.pressure_active = h_p.data_ptr(), h_pa.data_ptr()
+        h2d = (h_fluid.numel() * 4 + h_fact.numel() + h_solid.numel() * 4 + h_sact.numel()
+               + sum(v.numel() * 5 for v in h_vel))
+        d2h = sum(v.numel() * 5 for v in h_vel) + h_p.numel() * 5
+        e2e_steps = args.e2e_steps or args.steps
+        tot = 0.0
+        hres = native.Result()
+        for i in range(e2e_steps + 1):
+            for d in range(3):
+                h_vel[d].numpy()[...] = h_vel0[d]
+                h_vact[d].numpy()[...] = h_vact0[d]
+            rc = L.shkz_b200_project_host(ctx.handle, ctypes.byref(ha), ctypes.byref(hres))
+            if rc != 0:
+                raise native.ShkzError(rc, "shkz_b200_project_host", ctx.last_error())
+            if i > 0:  # first call is the warm-up
+                tot += hres.ms_total
+        e2e = {"value": tot / e2e_steps, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
+               "h2d_ms": hres.ms_h2d, "d2h_ms": hres.ms_d2h}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_reference_sample(128)
+        except Exception as exc:  # reported, not hidden
+            cpu = {"error": str(exc)}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": value, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (f64 reductions, refinement and assembly)", "data": "synthetic",
+            "config": {"workload": f"sloshing_tank {nx}^3, plain MIC(0)-PCG projection to 1e-6 (inf-norm), "
+                                   f"FP64 refinement, seed 0", "preconditioner": args.precond,
+                       "unknowns": last["unknowns"], "pool_tiles": last["tiles"],
+                       "l2": "inputs 0.42 GB and pool arrays > 126 MB L2 (no flush needed)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "step": "device velocity restore + one projection"},
+            "iterations": last["iterations"], "outer_steps": last["outer_steps"],
+            "reresid_inf": last["reresid"], "reresid_l2": last["reresid_l2"],
+            "phase_ms": {"assemble": last["ms_assemble"], "solve": last["ms_solve"], "update": last["ms_update"]},
+            "ms_per_iteration": last["ms_solve"] / max(1, last["iterations"]),
+            "e2e": e2e, "roofline": roofline, "kernels": kern, "cpu_baseline": cpu, "clocks": clocks,
+            "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,183 @@
+/*
+ * shkz_b200.h -- C ABI of the B200 MAC pressure projection.
+ *
+ * This is the boundary between host code written against Shiokaze's module
+ * API and the sm_100a CUDA implementation. Signatures use plain pointers and
+ * sizes only; no CUDA, C++ or torch types cross it. Every function returns
+ * 0 on success or a negative SHKZ_B200_ERR_* code, never throws and never
+ * exits the process.
+ *
+ * Reference interfaces replaced (paths relative to the Shiokaze tree):
+ *   shkz_b200_project*   macproject3_interface::project
+ *                        (include/shiokaze/projection/macproject3_interface.h:84-91),
+ *                        implemented by macpressuresolver3::project
+ *                        (src/projection/macpressuresolver3.cpp:54-299)
+ *   shkz_b200_solve_csr  RCMatrix_solver_interface<size_t,double>::solve
+ *                        (include/shiokaze/linsolver/RCMatrix_solver.h:44-77),
+ *                        implemented by pcg_solver::solve
+ *                        (src/linsolver/pcg.cpp:45-73)
+ *   shkz_b200_config     the configuration keys those modules read:
+ *                        Residual, MaxIterations, ModifiedIC, MinDiagRatio
+ *                        (src/linsolver/pcg.cpp:39-44), EpsFluid, EpsSolid
+ *                        (src/utility/macutility3.cpp:503-504),
+ *                        SecondOrderAccurateFluid/Solid
+ *                        (src/projection/macpressuresolver3.cpp:301-307)
+ *
+ * Grid conventions (same as the reference array3/macarray3 index space):
+ *   cells      nx*ny*nz, index i + nx*(j + ny*k)
+ *   nodes      (nx+1)*(ny+1)*(nz+1)            (solid level set)
+ *   faces dim0 (nx+1)*ny*nz, dim1 nx*(ny+1)*nz, dim2 nx*ny*(nz+1)
+ * Level-set and velocity inputs are the values array3::operator() returns
+ * for every cell (active value, fill value or background), plus one byte per
+ * cell that is 1 where the reference grid holds an active value.
+ */
+#ifndef SHKZ_B200_H
+#define SHKZ_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SHKZ_B200_ABI_VERSION 1
+
+enum {
+  SHKZ_B200_OK = 0,
+  SHKZ_B200_ERR_ARG = -1,        /* bad argument (null pointer, size) */
+  SHKZ_B200_ERR_CUDA = -2,       /* CUDA runtime error; see shkz_b200_last_error */
+  SHKZ_B200_ERR_NOMEM = -3,      /* device allocation failed */
+  SHKZ_B200_ERR_TIMEOUT = -4,    /* a bounded device wait gave up */
+  SHKZ_B200_ERR_NAN = -5,        /* NaN in the system or the iterates */
+  SHKZ_B200_ERR_NODEVICE = -6,   /* no usable sm_100 device */
+  SHKZ_B200_ERR_STATE = -7,      /* call order (e.g. no model loaded) */
+  SHKZ_B200_ERR_LIMIT = -8       /* size beyond a documented limit */
+};
+
+/* Preconditioner choice. NONE is what the shipped reference runs (its
+ * MIC(0) result is discarded, local/include/pcgsolver/pcg_solver.h:379-384);
+ * MIC0 applies the reference's own MIC(0) factor (pcg_solver.h:88-223);
+ * LEARNED is the conv-net preconditioner inside flexible PCG with MIC(0)
+ * fallback. */
+enum { SHKZ_B200_PRECOND_NONE = 0, SHKZ_B200_PRECOND_MIC0 = 1, SHKZ_B200_PRECOND_LEARNED = 2 };
+
+typedef struct shkz_b200_config {
+  double residual;            /* Residual (default 1e-4): stop at ||r||inf <= residual*||b||inf */
+  int max_iterations;         /* MaxIterations (default 30000) */
+  int preconditioner;         /* SHKZ_B200_PRECOND_* (default MIC0) */
+  double mic_omega;           /* ModifiedIC (default 0.97) */
+  double mic_min_diag_ratio;  /* MinDiagRatio (default 0.25) */
+  double eps_fluid;           /* EpsFluid (default 1e-2) */
+  double eps_solid;           /* EpsSolid (default 1e-2) */
+  int second_order_fluid;     /* SecondOrderAccurateFluid (default 1) */
+  int second_order_solid;     /* SecondOrderAccurateSolid (default 1) */
+  int refine;                 /* FP64 outer refinement of the FP32 solve (default 1) */
+  int fp64_reference;         /* also run an FP64 tight solve and report the error (default 0) */
+  double fp64_tol;            /* tolerance of that solve (default 1e-12) */
+  int check_interval;         /* iterations per device-side batch between host checks (default 16) */
+  int stall_window;           /* learned FPCG: iterations without progress before MIC(0) fallback */
+  int device;                 /* CUDA device ordinal (default 0) */
+  int reserved[8];
+} shkz_b200_config;
+
+/* Fill *cfg with the defaults listed above. */
+void shkz_b200_default_config(shkz_b200_config *cfg);
+
+typedef struct shkz_b200_ctx shkz_b200_ctx;
+
+int shkz_b200_create(shkz_b200_ctx **out, const shkz_b200_config *cfg);
+void shkz_b200_destroy(shkz_b200_ctx *ctx);
+int shkz_b200_set_config(shkz_b200_ctx *ctx, const shkz_b200_config *cfg);
+const char *shkz_b200_errstr(int code);
+/* Text of the last CUDA error seen by this thread's context, or "". */
+const char *shkz_b200_last_error(shkz_b200_ctx *ctx);
+
+/* Arguments of one projection: project(dt, velocity, solid, solid_velocity,
+ * fluid) of macproject3_interface. All arrays are either all host pointers
+ * (shkz_b200_project_host) or all device pointers (shkz_b200_project_device).
+ * solid / solid_active may be NULL for "no solid level set" (the reference's
+ * solid cleared to 1); solid_velocity may be NULL for zero solid velocity.
+ * velocity[] and velocity_active[] are updated in place; pressure (cells) and
+ * pressure_active (cells, 1 where an unknown was solved) are written. */
+typedef struct shkz_b200_project_args {
+  int nx, ny, nz;
+  double dx, dt;
+  const float *fluid;                  /* cells */
+  const uint8_t *fluid_active;         /* cells */
+  const float *solid;                  /* nodes, may be NULL */
+  const uint8_t *solid_active;         /* nodes, may be NULL */
+  float *velocity[3];                  /* faces, in/out */
+  uint8_t *velocity_active[3];         /* faces, in/out */
+  const float *solid_velocity[3];      /* faces, each may be NULL */
+  float *pressure;                     /* cells, out, may be NULL */
+  uint8_t *pressure_active;            /* cells, out, may be NULL */
+} shkz_b200_project_args;
+
+typedef struct shkz_b200_result {
+  int status;                /* 0 or SHKZ_B200_ERR_* */
+  int iterations;            /* total inner PCG iterations (reference: Result.count) */
+  int outer_steps;           /* FP64 refinement passes */
+  int fallbacks;             /* learned FPCG -> MIC(0) fallbacks */
+  long long unknowns;        /* number of pressure unknowns */
+  long long tiles;           /* tiles in the pool (8^3 tiles with >= 1 unknown) */
+  double reresid;            /* true ||r||inf/||b||inf after the solve (reference: Result.reresid) */
+  double reresid_l2;         /* true ||r||2/||b||2 */
+  double err_fp64_inf;       /* ||x - x_fp64||inf/||x_fp64||inf when fp64_reference, else -1 */
+  double fp64_reresid;       /* reached residual of the FP64 tight solve, else -1 */
+  double ms_assemble;        /* device time per phase (CUDA events) */
+  double ms_solve;
+  double ms_update;
+  double ms_total;
+  double ms_h2d, ms_d2h;     /* host paths only */
+  long long kernel_launches; /* CUDA kernels this library launched for the call */
+  double reserved[7];
+} shkz_b200_result;
+
+/* One pressure projection with host buffers: uploads, assembles, solves,
+ * updates the velocities and downloads. Host arrays may be pageable; pinned
+ * memory copies faster. */
+int shkz_b200_project_host(shkz_b200_ctx *ctx, const shkz_b200_project_args *args, shkz_b200_result *out);
+
+/* Same, with every array already resident on the context's device. */
+int shkz_b200_project_device(shkz_b200_ctx *ctx, const shkz_b200_project_args *args, shkz_b200_result *out);
+
+/* The CUDA stream the context launches on (as an opaque pointer), so callers
+ * can order their own work against it. */
+void *shkz_b200_stream(shkz_b200_ctx *ctx);
+
+/* Generic solver path for LinSolver=: solves A x = b for a symmetric CSR
+ * matrix given on the host (row-sorted, 0-based, FP64), same stopping rule
+ * as the reference PCG, MIC(0) computed on the device from the CSR. */
+int shkz_b200_solve_csr(shkz_b200_ctx *ctx, long long n, const long long *indptr, const long long *indices,
+                        const double *data, const double *b, double *x, shkz_b200_result *out);
+
+/* Inspection of the last projection's device state in dense grid layout
+ * (host buffers). what: 0 = diagonal (f32 cells), 1..3 = lower off-diagonal
+ * x/y/z (f32 cells), 4 = MIC(0) inverse pivot d (f32 cells), 5 = rhs (f64 cells),
+ * 6 = pressure (f64 cells, FP64 iterate), 7 = FP64 reference solution (f64 cells). */
+int shkz_b200_inspect(shkz_b200_ctx *ctx, int what, void *host_out, size_t bytes);
+
+/* Apply the preconditioner selected in the config once to a dense host
+ * residual (f32 cells) of the last projection's system and return z (f32
+ * cells); used to check the MIC(0) sweeps against a CPU restatement. */
+int shkz_b200_apply_preconditioner(shkz_b200_ctx *ctx, const float *r_cells, float *z_cells);
+
+/* y = A x on the last projection's system, dense f32 cells in and out. */
+int shkz_b200_apply_matrix(shkz_b200_ctx *ctx, const float *x_cells, float *y_cells);
+
+/* Device timing of one kernel on the last projection's system: launches it
+ * `reps` times on the context stream between CUDA events and stores the mean
+ * milliseconds per launch. which: 0 = stencil q = A p with fused p.q,
+ * 1 = MIC(0) forward sweep, 2 = MIC(0) backward sweep with fused z.r,
+ * 3 = fused x/r update with norms, 4 = p update, 5 = unknown labelling,
+ * 6 = weights/rhs assembly, 7 = MIC(0) factor. *cells_out (may be NULL)
+ * receives the cells the kernel sweeps per launch (pool cells, or grid cells
+ * for 5). No reference counterpart: it is the measurement hook for the
+ * roofline figures. */
+int shkz_b200_time_kernel(shkz_b200_ctx *ctx, int which, int reps, double *ms_per_launch, long long *cells_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,64 @@
+"""Build the sm_100a CUDA library ``libshkz_b200.so`` in-tree with nvcc.
+
+    python -m shiokaze_b200.build          # or build() from Python
+
+Every translation unit is compiled for sm_100a only
+(``-gencode arch=compute_100a,code=sm_100a``); the assembly unit is compiled
+with ``-fmad=false`` so its FP64 face arithmetic rounds like the reference's
+CPU code. The CUDA runtime is linked statically so the library does not
+depend on which libcudart the host process already loaded.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libshkz_b200.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
+          "--expt-relaxed-constexpr", "-I" + os.path.join(HERE, "..", "include")]
+UNITS = {
+    "assemble.cu": ["-fmad=false"],
+    "solver.cu": [],
+    "learned.cu": [],
+    "api.cu": [],
+}
+HEADERS = ["common.cuh", "kernels.h", "solver.h", "learned.h"]
+
+
+def _stale(target: str, deps) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def build(verbose: bool = False, extra=None) -> str:
+    os.makedirs(BUILD, exist_ok=True)
+    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(HERE, "..", "include", "shkz_b200.h")]
+    objs = []
+    for unit, flags in UNITS.items():
+        src = os.path.join(CSRC, unit)
+        obj = os.path.join(BUILD, unit.replace(".cu", ".o"))
+        objs.append(obj)
+        if _stale(obj, [src] + hdrs):
+            cmd = [NVCC] + ARCH + COMMON + flags + (extra or []) + ["-c", src, "-o", obj]
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            subprocess.check_call(cmd)
+    if _stale(LIB, objs):
+        cmd = [NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", LIB] + objs
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.check_call(cmd)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(verbose=True, extra=sys.argv[1:])

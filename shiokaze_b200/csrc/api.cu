@@ -1,0 +1,954 @@
+// C ABI of the B200 pressure projection (declared in include/shkz_b200.h).
+//
+// One context owns one CUDA stream and every device buffer; nothing is
+// allocated per iteration. A projection runs:
+//   label unknowns -> build the 8^3 tile pool -> weights/rhs -> MIC(0) factor
+//   -> FP32 PCG with FP64 reductions inside an FP64 refinement loop
+//   -> pressure scatter and velocity update.
+// The PCG runs in batches of `check_interval` iterations; each kernel reads
+// the device-side solver state and returns at once after convergence, so the
+// host only synchronises once per batch.
+#include "common.cuh"
+#include "kernels.h"
+#include "solver.h"
+#include "learned.h"
+#include "../../include/shkz_b200.h"
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace shkz;
+
+static thread_local char g_last_error[512] = {0};
+
+void shkz_set_cuda_error(cudaError_t e, const char *expr, const char *file, int line) {
+  std::snprintf(g_last_error, sizeof(g_last_error), "%s (%d) at %s:%d: %s", cudaGetErrorString(e), (int)e, file, line,
+                expr);
+}
+
+struct shkz_b200_ctx {
+  shkz_b200_config cfg;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[8] = {};
+  // dense capacities
+  size_t cap_cells = 0;
+  size_t cap_h_cells = 0, cap_h_nodes = 0, cap_h_faces[3] = {0, 0, 0};
+  long long cap_tiles = 0;
+  int cap_pool = 0;
+  // dense staging buffers for the host path
+  float *h_fluid = nullptr, *h_solid = nullptr, *h_vel[3] = {}, *h_svel[3] = {}, *h_pressure = nullptr;
+  uint8_t *h_fluid_active = nullptr, *h_solid_active = nullptr, *h_vact[3] = {}, *h_pact = nullptr;
+  // assembly
+  int *flags = nullptr;
+  uint8_t *unk = nullptr;
+  int *tile_count = nullptr, *tile_state = nullptr, *pool_tile = nullptr, *nbr = nullptr, *level_count = nullptr,
+      *sched = nullptr, *bsum = nullptr, *total = nullptr;
+  // pool arrays
+  float *diag = nullptr, *offx = nullptr, *offy = nullptr, *offz = nullptr, *d32 = nullptr;
+  double *diag64 = nullptr, *offx64 = nullptr, *offy64 = nullptr, *offz64 = nullptr, *rhs64 = nullptr,
+         *colsum = nullptr, *dmic64 = nullptr, *x64 = nullptr, *r64 = nullptr, *xref64 = nullptr,
+         *p64 = nullptr, *q64 = nullptr, *z64 = nullptr;
+  float *x = nullptr, *r = nullptr, *p = nullptr, *q = nullptr, *z = nullptr, *t = nullptr, *p32 = nullptr;
+  // reductions and wavefront sync
+  double *partials = nullptr, *out4 = nullptr;
+  unsigned *counter = nullptr;
+  SolverState *st = nullptr;
+  int *wflags = nullptr;  // [3][cap_pool]
+  void *ws = nullptr;     // 3 WaveSync
+  // last projection
+  Geometry G{};
+  int K = 0;
+  long long unknowns = 0;
+  int has_system = 0;
+  LearnedModel *model = nullptr;
+  AssemblyInputs last_in{};
+  SolverState *st_scratch = nullptr;
+};
+
+extern "C" void shkz_b200_default_config(shkz_b200_config *c) {
+  std::memset(c, 0, sizeof(*c));
+  c->residual = 1e-4;
+  c->max_iterations = 30000;
+  c->preconditioner = SHKZ_B200_PRECOND_MIC0;
+  c->mic_omega = 0.97;
+  c->mic_min_diag_ratio = 0.25;
+  c->eps_fluid = 1e-2;
+  c->eps_solid = 1e-2;
+  c->second_order_fluid = 1;
+  c->second_order_solid = 1;
+  c->refine = 1;
+  c->fp64_reference = 0;
+  c->fp64_tol = 1e-12;
+  c->check_interval = 16;
+  c->stall_window = 8;
+  c->device = 0;
+}
+
+extern "C" const char *shkz_b200_errstr(int code) {
+  switch (code) {
+    case SHKZ_B200_OK: return "ok";
+    case SHKZ_B200_ERR_ARG: return "invalid argument";
+    case SHKZ_B200_ERR_CUDA: return "CUDA runtime error";
+    case SHKZ_B200_ERR_NOMEM: return "device allocation failed";
+    case SHKZ_B200_ERR_TIMEOUT: return "a bounded device wait gave up";
+    case SHKZ_B200_ERR_NAN: return "NaN in the system or the iterates";
+    case SHKZ_B200_ERR_NODEVICE: return "no usable sm_100 device";
+    case SHKZ_B200_ERR_STATE: return "invalid call order";
+    case SHKZ_B200_ERR_LIMIT: return "size beyond a documented limit";
+    default: return "unknown error";
+  }
+}
+
+extern "C" const char *shkz_b200_last_error(shkz_b200_ctx *) { return g_last_error; }
+
+template <class T>
+static int grow(T **ptr, size_t need, size_t &cap_dummy) {
+  (void)cap_dummy;
+  if (*ptr) cudaFree(*ptr);
+  *ptr = nullptr;
+  if (need == 0) return 0;
+  cudaError_t e = cudaMalloc((void **)ptr, need * sizeof(T));
+  if (e != cudaSuccess) {
+    shkz_set_cuda_error(e, "cudaMalloc", __FILE__, __LINE__);
+    *ptr = nullptr;
+    return SHKZ_B200_ERR_NOMEM;
+  }
+  return 0;
+}
+
+#define GROW(field, n)                                  \
+  do {                                                  \
+    size_t _d = 0;                                      \
+    int _rc = grow(&ctx->field, (size_t)(n), _d);       \
+    if (_rc) return _rc;                                \
+  } while (0)
+
+static Geometry make_geometry(int nx, int ny, int nz) {
+  Geometry G;
+  G.nx = nx;
+  G.ny = ny;
+  G.nz = nz;
+  G.bx = (nx + SHKZ_T - 1) / SHKZ_T;
+  G.by = (ny + SHKZ_T - 1) / SHKZ_T;
+  G.bz = (nz + SHKZ_T - 1) / SHKZ_T;
+  G.ntiles = (long long)G.bx * G.by * G.bz;
+  return G;
+}
+
+static int ensure_grid(shkz_b200_ctx *ctx, const Geometry &G) {
+  const size_t cells = (size_t)G.nx * G.ny * G.nz;
+  if (cells > ctx->cap_cells) {
+    GROW(unk, cells);
+    ctx->cap_cells = cells;
+  }
+  if (G.ntiles > ctx->cap_tiles) {
+    GROW(tile_count, G.ntiles);
+    GROW(tile_state, G.ntiles);
+    GROW(bsum, (G.ntiles + 1023) / 1024 + 1);
+    ctx->cap_tiles = G.ntiles;
+  }
+  if (!ctx->level_count) {
+    // levels bx+by+bz <= 3 * 65536 / 8 for any grid this ABI accepts
+    GROW(level_count, 3 * 8192 + 8);
+  }
+  return 0;
+}
+
+static int ensure_host_staging(shkz_b200_ctx *ctx, const Geometry &G, bool solid, const bool svel[3]) {
+  const size_t cells = (size_t)G.nx * G.ny * G.nz;
+  const size_t nodes = (size_t)(G.nx + 1) * (G.ny + 1) * (G.nz + 1);
+  if (cells > ctx->cap_h_cells) {
+    GROW(h_fluid, cells);
+    GROW(h_fluid_active, cells);
+    GROW(h_pressure, cells);
+    GROW(h_pact, cells);
+    ctx->cap_h_cells = cells;
+  }
+  if (solid && nodes > ctx->cap_h_nodes) {
+    GROW(h_solid, nodes);
+    GROW(h_solid_active, nodes);
+    ctx->cap_h_nodes = nodes;
+  }
+  for (int d = 0; d < 3; ++d) {
+    const size_t nf = (size_t)(G.nx + (d == 0)) * (G.ny + (d == 1)) * (G.nz + (d == 2));
+    if (nf > ctx->cap_h_faces[d]) {
+      GROW(h_vel[d], nf);
+      GROW(h_vact[d], nf);
+      if (ctx->h_svel[d]) { cudaFree(ctx->h_svel[d]); ctx->h_svel[d] = nullptr; }
+      ctx->cap_h_faces[d] = nf;
+    }
+    if (svel[d] && !ctx->h_svel[d]) GROW(h_svel[d], ctx->cap_h_faces[d]);
+  }
+  return 0;
+}
+
+static int ensure_pool(shkz_b200_ctx *ctx, int K) {
+  if (K <= ctx->cap_pool) return 0;
+  int cap = K + K / 4 + 16;
+  const size_t n = (size_t)cap * SHKZ_TC;
+  GROW(pool_tile, cap);
+  GROW(nbr, (size_t)cap * 6);
+  GROW(sched, cap);
+  GROW(diag, n); GROW(offx, n); GROW(offy, n); GROW(offz, n); GROW(d32, n);
+  GROW(diag64, n); GROW(offx64, n); GROW(offy64, n); GROW(offz64, n); GROW(rhs64, n);
+  GROW(colsum, n); GROW(dmic64, n); GROW(x64, n); GROW(r64, n); GROW(xref64, n);
+  GROW(p64, n); GROW(q64, n); GROW(z64, n);
+  GROW(x, n); GROW(r, n); GROW(p, n); GROW(q, n); GROW(z, n); GROW(t, n); GROW(p32, n);
+  GROW(partials, (size_t)cap + 4 * 8192);
+  GROW(wflags, (size_t)3 * cap);
+  SHKZ_CUDA_TRY(cudaMemsetAsync(ctx->wflags, 0, sizeof(int) * 3 * (size_t)cap, ctx->stream));
+  if (ctx->ws) {
+    // flags were reset: restart the epochs
+    SHKZ_CUDA_TRY(cudaMemsetAsync(ctx->ws, 0, 3 * wave_sync_bytes(), ctx->stream));
+  }
+  ctx->cap_pool = cap;
+  return 0;
+}
+
+extern "C" int shkz_b200_create(shkz_b200_ctx **out, const shkz_b200_config *cfg) {
+  if (!out) return SHKZ_B200_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return SHKZ_B200_ERR_NODEVICE;
+  shkz_b200_ctx *ctx = new shkz_b200_ctx();
+  if (cfg) ctx->cfg = *cfg;
+  else shkz_b200_default_config(&ctx->cfg);
+  ctx->device = ctx->cfg.device;
+  if (ctx->device < 0 || ctx->device >= ndev) {
+    delete ctx;
+    return SHKZ_B200_ERR_ARG;
+  }
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, ctx->device) != cudaSuccess || prop.major < 10) {
+    delete ctx;
+    return SHKZ_B200_ERR_NODEVICE;
+  }
+  cudaSetDevice(ctx->device);
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete ctx;
+    return SHKZ_B200_ERR_CUDA;
+  }
+  for (auto &e : ctx->ev) cudaEventCreate(&e);
+  if (cudaMalloc(&ctx->flags, sizeof(int)) != cudaSuccess || cudaMalloc(&ctx->total, sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&ctx->counter, sizeof(unsigned) * 8) != cudaSuccess ||
+      cudaMalloc(&ctx->st, sizeof(SolverState)) != cudaSuccess || cudaMalloc(&ctx->out4, sizeof(double) * 8) != cudaSuccess ||
+      cudaMalloc(&ctx->ws, 3 * wave_sync_bytes()) != cudaSuccess ||
+      cudaMalloc(&ctx->st_scratch, sizeof(SolverState)) != cudaSuccess) {
+    shkz_b200_destroy(ctx);
+    return SHKZ_B200_ERR_NOMEM;
+  }
+  cudaMemsetAsync(ctx->counter, 0, sizeof(unsigned) * 8, ctx->stream);
+  cudaMemsetAsync(ctx->ws, 0, 3 * wave_sync_bytes(), ctx->stream);
+  cudaMemsetAsync(ctx->st, 0, sizeof(SolverState), ctx->stream);
+  if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+    shkz_b200_destroy(ctx);
+    return SHKZ_B200_ERR_CUDA;
+  }
+  *out = ctx;
+  return 0;
+}
+
+extern "C" void shkz_b200_destroy(shkz_b200_ctx *ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  void *ptrs[] = {ctx->h_fluid, ctx->h_solid, ctx->h_vel[0], ctx->h_vel[1], ctx->h_vel[2], ctx->h_svel[0],
+                  ctx->h_svel[1], ctx->h_svel[2], ctx->h_pressure, ctx->h_fluid_active, ctx->h_solid_active,
+                  ctx->h_vact[0], ctx->h_vact[1], ctx->h_vact[2], ctx->h_pact, ctx->flags, ctx->unk, ctx->tile_count,
+                  ctx->tile_state, ctx->pool_tile, ctx->nbr, ctx->level_count, ctx->sched, ctx->bsum, ctx->total,
+                  ctx->diag, ctx->offx, ctx->offy, ctx->offz, ctx->d32, ctx->diag64, ctx->offx64, ctx->offy64,
+                  ctx->offz64, ctx->rhs64, ctx->colsum, ctx->dmic64, ctx->x64, ctx->r64, ctx->xref64, ctx->p64, ctx->q64,
+                  ctx->z64, ctx->x, ctx->r,
+                  ctx->p, ctx->q, ctx->z, ctx->t, ctx->p32, ctx->partials, ctx->out4, ctx->counter, ctx->st,
+                  ctx->wflags, ctx->ws, ctx->st_scratch};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (ctx->model) learned_free(ctx->model);
+  for (auto &e : ctx->ev)
+    if (e) cudaEventDestroy(e);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+extern "C" int shkz_b200_set_config(shkz_b200_ctx *ctx, const shkz_b200_config *cfg) {
+  if (!ctx || !cfg) return SHKZ_B200_ERR_ARG;
+  ctx->cfg = *cfg;
+  return 0;
+}
+
+extern "C" void *shkz_b200_stream(shkz_b200_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+static PoolSystem pool_system(shkz_b200_ctx *ctx) {
+  PoolSystem S;
+  S.K = ctx->K;
+  S.nbr = ctx->nbr;
+  S.sched = ctx->sched;
+  S.diag = ctx->diag;
+  S.offx = ctx->offx;
+  S.offy = ctx->offy;
+  S.offz = ctx->offz;
+  S.diag64 = ctx->diag64;
+  S.offx64 = ctx->offx64;
+  S.offy64 = ctx->offy64;
+  S.offz64 = ctx->offz64;
+  return S;
+}
+
+static char *wsync(shkz_b200_ctx *ctx, int which) { return (char *)ctx->ws + which * wave_sync_bytes(); }
+
+// Wave-sync error word (offset of `error` inside WaveSync is 3 ints).
+static int wave_errors(shkz_b200_ctx *ctx) {
+  std::vector<char> h(3 * wave_sync_bytes());
+  if (cudaMemcpy(h.data(), ctx->ws, h.size(), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+  int any = 0;
+  for (int w = 0; w < 3; ++w) {
+    int err;
+    std::memcpy(&err, h.data() + w * wave_sync_bytes() + 3 * sizeof(int), sizeof(int));
+    any |= (err != 0);
+  }
+  return any;
+}
+
+// --------------------------------------------------------------------------
+// Inner FP32 PCG on (A32, r, x): the reference loop, batched.
+// Returns iterations; *done_code gets the solver's done value.
+static int inner_pcg(shkz_b200_ctx *ctx, double tol, int max_it, int precond, int *done_code) {
+  cudaStream_t s = ctx->stream;
+  const PoolSystem S = pool_system(ctx);
+  const int n = ctx->K * SHKZ_TC;
+  launch_inner_setup(n, ctx->r, ctx->partials, ctx->counter, ctx->st, tol, s);
+  // z = M^-1 r, rho = z.r, p = z
+  if (precond == SHKZ_B200_PRECOND_MIC0) {
+    launch_mic_apply(S, ctx->d32, ctx->r, ctx->t, ctx->z, ctx->partials, ctx->wflags + ctx->cap_pool,
+                     ctx->wflags + 2 * ctx->cap_pool, wsync(ctx, 1), wsync(ctx, 2), ctx->st, s);
+    launch_finish_rho(ctx->partials, ctx->K, ctx->st, 1, s);
+    cudaMemcpyAsync(ctx->p, ctx->z, sizeof(float) * n, cudaMemcpyDeviceToDevice, s);
+  } else {
+    launch_finish_rho_r2(ctx->st, 1, s);
+    cudaMemcpyAsync(ctx->p, ctx->r, sizeof(float) * n, cudaMemcpyDeviceToDevice, s);
+  }
+  const int batch = ctx->cfg.check_interval > 0 ? ctx->cfg.check_interval : 16;
+  SolverState hst;
+  int launched = 0;
+  for (;;) {
+    for (int b = 0; b < batch && launched < max_it; ++b, ++launched) {
+      launch_spmv(S, ctx->p, ctx->q, ctx->partials, ctx->counter, ctx->st, 0, s);
+      launch_update_xr(n, ctx->p, ctx->q, ctx->x, ctx->r, ctx->partials, ctx->counter + 1, ctx->st, max_it, s);
+      if (precond == SHKZ_B200_PRECOND_MIC0) {
+        launch_mic_apply(S, ctx->d32, ctx->r, ctx->t, ctx->z, ctx->partials, ctx->wflags + ctx->cap_pool,
+                         ctx->wflags + 2 * ctx->cap_pool, wsync(ctx, 1), wsync(ctx, 2), ctx->st, s);
+        launch_finish_rho(ctx->partials, ctx->K, ctx->st, 0, s);
+        launch_update_p(n, ctx->z, ctx->p, ctx->st, s);
+      } else {
+        launch_finish_rho_r2(ctx->st, 0, s);
+        launch_update_p(n, ctx->r, ctx->p, ctx->st, s);
+      }
+    }
+    if (cudaMemcpyAsync(&hst, ctx->st, sizeof(hst), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+      shkz_set_cuda_error(cudaGetLastError(), "inner_pcg sync", __FILE__, __LINE__);
+      *done_code = -1;
+      return -1;
+    }
+    if (hst.done || launched >= max_it) break;
+  }
+  *done_code = hst.done;
+  if (hst.status == -5) *done_code = 3;
+  return hst.iter;
+}
+
+// FP64 refinement around the FP32 PCG. x64 holds the solution on return.
+static int solve_system(shkz_b200_ctx *ctx, double tol, int precond, shkz_b200_result *res) {
+  cudaStream_t s = ctx->stream;
+  const PoolSystem S = pool_system(ctx);
+  const int n = ctx->K * SHKZ_TC;
+  SHKZ_CUDA_TRY(cudaMemsetAsync(ctx->x64, 0, sizeof(double) * n, s));
+  double h4[4];
+  launch_residual64(S, ctx->rhs64, ctx->x64, ctx->r64, ctx->partials, ctx->counter + 2, ctx->out4, s);
+  SHKZ_CUDA_TRY(cudaMemcpyAsync(h4, ctx->out4, sizeof(h4), cudaMemcpyDeviceToHost, s));
+  SHKZ_CUDA_TRY(cudaStreamSynchronize(s));
+  const double bmax = h4[2], b2 = h4[3];
+  double rmax = h4[0], r2 = h4[1];
+  int iterations = 0, outer = 0, rc = 0;
+  if (bmax == 0.0) {
+    res->iterations = 0;
+    res->reresid = 0.0;
+    res->reresid_l2 = 0.0;
+    res->outer_steps = 0;
+    return 0;
+  }
+  const int max_outer = ctx->cfg.refine ? 12 : 1;
+  while (outer < max_outer) {
+    const double scale = rmax;
+    // inner relative tolerance: the target itself on the first pass, then
+    // what is left to gain (bounded below by what FP32 iterates can reach)
+    double tol_inner = (outer == 0) ? tol : std::fmax(0.5 * tol * bmax / rmax, 2e-6);
+    if (tol_inner > 0.5) tol_inner = 0.5;
+    launch_inner_init(n, ctx->r64, 1.0 / scale, ctx->r, ctx->x, s);
+    int done = 0;
+    const int it = inner_pcg(ctx, tol_inner, ctx->cfg.max_iterations - iterations, precond, &done);
+    if (it < 0) return SHKZ_B200_ERR_CUDA;
+    iterations += it;
+    launch_accumulate(n, ctx->x, scale, ctx->x64, s);
+    launch_residual64(S, ctx->rhs64, ctx->x64, ctx->r64, ctx->partials, ctx->counter + 2, ctx->out4, s);
+    SHKZ_CUDA_TRY(cudaMemcpyAsync(h4, ctx->out4, sizeof(h4), cudaMemcpyDeviceToHost, s));
+    SHKZ_CUDA_TRY(cudaStreamSynchronize(s));
+    rmax = h4[0];
+    r2 = h4[1];
+    ++outer;
+    if (done == 3 || !(rmax == rmax)) { rc = SHKZ_B200_ERR_NAN; break; }
+    if (!ctx->cfg.refine) break;
+    if (rmax <= tol * bmax) break;
+    if (iterations >= ctx->cfg.max_iterations) break;
+    if (done == 2) break;
+  }
+  if (wave_errors(ctx)) rc = SHKZ_B200_ERR_TIMEOUT;
+  res->iterations = iterations;
+  res->outer_steps = outer;
+  res->reresid = rmax / bmax;
+  res->reresid_l2 = std::sqrt(r2 / b2);
+  return rc;
+}
+
+// FP64 tight reference solve: flexible CG (Polak-Ribiere beta) in FP64 whose
+// preconditioner is the FP32 MIC(0) applied to the scaled residual. It
+// solves the same FP64 system the reference assembles, to fp64_tol, into
+// xref64, and reports ||x64 - xref64||inf / ||xref64||inf.
+static int fp64_reference_solve(shkz_b200_ctx *ctx, shkz_b200_result *res) {
+  cudaStream_t s = ctx->stream;
+  const PoolSystem S = pool_system(ctx);
+  const int n = ctx->K * SHKZ_TC;
+  const double tol = ctx->cfg.fp64_tol > 0 ? ctx->cfg.fp64_tol : 1e-12;
+  double h[4];
+  auto dots = [&](const double *a, const double *b, const double *c, const double *d) -> int {
+    launch_dots64(n, a, b, c, d, ctx->partials, ctx->counter + 3, ctx->out4, s);
+    if (cudaMemcpyAsync(h, ctx->out4, sizeof(double) * 3, cudaMemcpyDeviceToHost, s) != cudaSuccess) return -1;
+    return cudaStreamSynchronize(s) == cudaSuccess ? 0 : -1;
+  };
+  auto precond = [&](const double *r, double rmax) {
+    // z = rmax * M^-1 (r / rmax) with M^-1 the FP32 MIC(0)
+    launch_scale_f64_f32(n, r, 1.0 / rmax, ctx->r, s);
+    launch_mic_apply(S, ctx->d32, ctx->r, ctx->t, ctx->z, nullptr, ctx->wflags + ctx->cap_pool,
+                     ctx->wflags + 2 * ctx->cap_pool, wsync(ctx, 1), wsync(ctx, 2), nullptr, s);
+    launch_scale_f32_f64(n, ctx->z, rmax, ctx->z64, s);
+  };
+  SHKZ_CUDA_TRY(cudaMemsetAsync(ctx->xref64, 0, sizeof(double) * n, s));
+  SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->r64, ctx->rhs64, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  if (dots(ctx->r64, ctx->r64, nullptr, nullptr)) return SHKZ_B200_ERR_CUDA;
+  const double bmax = h[2];
+  if (bmax == 0.0) {
+    res->fp64_reresid = 0.0;
+    res->err_fp64_inf = 0.0;
+    return 0;
+  }
+  double rmax = bmax;
+  precond(ctx->r64, rmax);
+  if (dots(ctx->z64, ctx->r64, nullptr, nullptr)) return SHKZ_B200_ERR_CUDA;
+  double rho = h[0];
+  SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->p64, ctx->z64, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  int it = 0;
+  const int max_it = ctx->cfg.max_iterations;
+  for (; it < max_it; ++it) {
+    launch_apply64(S, ctx->p64, ctx->q64, s);
+    if (dots(ctx->p64, ctx->q64, nullptr, nullptr)) return SHKZ_B200_ERR_CUDA;
+    const double alpha = rho / h[0];
+    launch_axpy2_64(n, alpha, ctx->p64, ctx->xref64, ctx->q64, ctx->r64, s);
+    if (dots(ctx->r64, ctx->r64, nullptr, nullptr)) return SHKZ_B200_ERR_CUDA;
+    rmax = h[2];
+    if (!(rmax == rmax)) return SHKZ_B200_ERR_NAN;
+    if (rmax <= tol * bmax) break;
+    precond(ctx->r64, rmax);
+    if (dots(ctx->z64, ctx->r64, ctx->z64, ctx->q64)) return SHKZ_B200_ERR_CUDA;
+    const double rho_new = h[0];
+    const double beta = -alpha * h[1] / rho;
+    launch_xpby64(n, ctx->z64, beta, ctx->p64, s);
+    rho = rho_new;
+  }
+  // true residual of the reference solution and the error of x64
+  launch_residual64(S, ctx->rhs64, ctx->xref64, ctx->r64, ctx->partials, ctx->counter + 2, ctx->out4, s);
+  SHKZ_CUDA_TRY(cudaMemcpyAsync(h, ctx->out4, sizeof(double) * 4, cudaMemcpyDeviceToHost, s));
+  SHKZ_CUDA_TRY(cudaStreamSynchronize(s));
+  res->fp64_reresid = h[0] / h[2];
+  // error: ||x64 - xref64||inf over ||xref64||inf  (q64 = x64 - xref64)
+  SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->q64, ctx->x64, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  launch_axpy2_64(n, -1.0, ctx->xref64, ctx->q64, ctx->xref64, ctx->p64, s);  // second pair is a scratch write
+  if (dots(ctx->q64, ctx->q64, ctx->xref64, ctx->xref64)) return SHKZ_B200_ERR_CUDA;
+  const double emax = h[2];
+  if (dots(ctx->xref64, ctx->xref64, nullptr, nullptr)) return SHKZ_B200_ERR_CUDA;
+  res->err_fp64_inf = h[2] > 0 ? emax / h[2] : 0.0;
+  return 0;
+}
+
+static int validate(const shkz_b200_project_args *a) {
+  if (!a || a->nx <= 0 || a->ny <= 0 || a->nz <= 0 || !a->fluid || !a->fluid_active) return SHKZ_B200_ERR_ARG;
+  if (a->nx > 65536 || a->ny > 65536 || a->nz > 65536) return SHKZ_B200_ERR_LIMIT;
+  if ((size_t)a->nx * a->ny * a->nz > ((size_t)1 << 31)) return SHKZ_B200_ERR_LIMIT;
+  if ((a->solid == nullptr) != (a->solid_active == nullptr)) return SHKZ_B200_ERR_ARG;
+  for (int d = 0; d < 3; ++d)
+    if (!a->velocity[d] || !a->velocity_active[d]) return SHKZ_B200_ERR_ARG;
+  if (!(a->dx > 0.0)) return SHKZ_B200_ERR_ARG;
+  return 0;
+}
+
+static float ms_between(cudaEvent_t a, cudaEvent_t b) {
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, a, b);
+  return ms;
+}
+
+static int project_device(shkz_b200_ctx *ctx, const shkz_b200_project_args *a, shkz_b200_result *res) {
+  cudaStream_t s = ctx->stream;
+  const Geometry G = make_geometry(a->nx, a->ny, a->nz);
+  int rc = ensure_grid(ctx, G);
+  if (rc) return rc;
+  AssemblyInputs in;
+  in.G = G;
+  in.fluid = a->fluid;
+  in.fluid_active = a->fluid_active;
+  in.solid = a->solid;
+  in.solid_active = a->solid_active;
+  for (int d = 0; d < 3; ++d) {
+    in.vel[d] = a->velocity[d];
+    in.svel[d] = a->solid_velocity[d];
+  }
+  in.dx = a->dx;
+  in.dt = a->dt;
+  in.eps_solid = ctx->cfg.eps_solid;
+  in.eps_fluid = ctx->cfg.eps_fluid;
+  in.second_order_fluid = ctx->cfg.second_order_fluid;
+  in.second_order_solid = ctx->cfg.second_order_solid;
+
+  ctx->last_in = in;
+  const long long launches0 = launches_so_far();
+  cudaEventRecord(ctx->ev[0], s);
+  launch_label(in, ctx->flags, ctx->unk, ctx->tile_count, s);
+  // pool size (one small host read), then the pool itself
+  const int K = pool_count(G, ctx->tile_count, ctx->bsum, ctx->total, s);
+  if (K < 0) {
+    shkz_set_cuda_error(cudaGetLastError(), "pool_count", __FILE__, __LINE__);
+    return SHKZ_B200_ERR_CUDA;
+  }
+  rc = ensure_pool(ctx, K > 0 ? K : 1);
+  if (rc) return rc;
+  pool_assign(G, ctx->tile_count, K, ctx->bsum, ctx->tile_state, ctx->pool_tile, ctx->nbr, ctx->level_count,
+              ctx->sched, s);
+  SHKZ_CUDA_TRY(cudaGetLastError());
+  ctx->K = K;
+  ctx->G = G;
+  res->tiles = K;
+  CoeffOutputs co{ctx->diag, ctx->offx, ctx->offy, ctx->offz, ctx->diag64, ctx->offx64, ctx->offy64, ctx->offz64,
+                  ctx->rhs64};
+  launch_coeff(in, ctx->flags, ctx->pool_tile, K, ctx->unk, co, s);
+  const int precond = ctx->cfg.preconditioner;
+  const PoolSystem S = pool_system(ctx);
+  if (K > 0 && (precond == SHKZ_B200_PRECOND_MIC0 || precond == SHKZ_B200_PRECOND_LEARNED))
+    launch_mic_factor(S, ctx->colsum, ctx->cfg.mic_omega, ctx->cfg.mic_min_diag_ratio, ctx->dmic64, ctx->d32,
+                      ctx->wflags, wsync(ctx, 0), s);
+  SHKZ_CUDA_TRY(cudaGetLastError());
+  cudaEventRecord(ctx->ev[1], s);
+  ctx->has_system = 1;
+  // unknown count (for the result)
+  {
+    std::vector<int> tc((size_t)G.ntiles);
+    SHKZ_CUDA_TRY(cudaMemcpyAsync(tc.data(), ctx->tile_count, sizeof(int) * G.ntiles, cudaMemcpyDeviceToHost, s));
+    SHKZ_CUDA_TRY(cudaStreamSynchronize(s));
+    long long u = 0;
+    for (int v : tc) u += v;
+    ctx->unknowns = u;
+    res->unknowns = u;
+  }
+  int solve_rc = 0;
+  if (K > 0) {
+    if (precond == SHKZ_B200_PRECOND_LEARNED && ctx->model)
+      solve_rc = learned_solve(ctx->model, ctx, res);
+    else
+      solve_rc = solve_system(ctx, ctx->cfg.residual, precond == SHKZ_B200_PRECOND_LEARNED ? SHKZ_B200_PRECOND_MIC0 : precond, res);
+  } else {
+    res->iterations = 0;
+    res->reresid = 0.0;
+  }
+  cudaEventRecord(ctx->ev[2], s);
+  // FP32 pressure of the solution, then the velocity update
+  const int n = K * SHKZ_TC;
+  if (K > 0) launch_to_float(n, ctx->x64, ctx->p32, s);
+  float *vel[3] = {a->velocity[0], a->velocity[1], a->velocity[2]};
+  uint8_t *vact[3] = {a->velocity_active[0], a->velocity_active[1], a->velocity_active[2]};
+  if (K > 0) launch_velocity_update(in, ctx->flags, ctx->tile_state, ctx->p32, vel, vact, s);
+  if (a->pressure || a->pressure_active)
+    launch_scatter_pressure(G, ctx->tile_state, ctx->p32, ctx->unk, a->pressure, a->pressure_active, s);
+  cudaEventRecord(ctx->ev[3], s);
+  SHKZ_CUDA_TRY(cudaGetLastError());
+  // optional FP64 tight reference solve
+  res->err_fp64_inf = -1.0;
+  res->fp64_reresid = -1.0;
+  if (K > 0 && ctx->cfg.fp64_reference) {
+    int rrc = fp64_reference_solve(ctx, res);
+    if (rrc && !solve_rc) solve_rc = rrc;
+  }
+  SHKZ_CUDA_TRY(cudaStreamSynchronize(s));
+  res->ms_assemble = ms_between(ctx->ev[0], ctx->ev[1]);
+  res->ms_solve = ms_between(ctx->ev[1], ctx->ev[2]);
+  res->ms_update = ms_between(ctx->ev[2], ctx->ev[3]);
+  res->ms_total = ms_between(ctx->ev[0], ctx->ev[3]);
+  res->kernel_launches = launches_so_far() - launches0;
+  res->status = solve_rc;
+  return solve_rc;
+}
+
+extern "C" int shkz_b200_project_device(shkz_b200_ctx *ctx, const shkz_b200_project_args *a, shkz_b200_result *res) {
+  if (!ctx || !res) return SHKZ_B200_ERR_ARG;
+  std::memset(res, 0, sizeof(*res));
+  int rc = validate(a);
+  if (rc) return res->status = rc;
+  cudaSetDevice(ctx->device);
+  rc = project_device(ctx, a, res);
+  res->status = rc;
+  return rc;
+}
+
+extern "C" int shkz_b200_project_host(shkz_b200_ctx *ctx, const shkz_b200_project_args *a, shkz_b200_result *res) {
+  if (!ctx || !res) return SHKZ_B200_ERR_ARG;
+  std::memset(res, 0, sizeof(*res));
+  int rc = validate(a);
+  if (rc) return res->status = rc;
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  const Geometry G = make_geometry(a->nx, a->ny, a->nz);
+  const bool svel[3] = {a->solid_velocity[0] != nullptr, a->solid_velocity[1] != nullptr,
+                        a->solid_velocity[2] != nullptr};
+  rc = ensure_grid(ctx, G);
+  if (rc) return res->status = rc;
+  rc = ensure_host_staging(ctx, G, a->solid != nullptr, svel);
+  if (rc) return res->status = rc;
+  const size_t cells = (size_t)G.nx * G.ny * G.nz;
+  const size_t nodes = (size_t)(G.nx + 1) * (G.ny + 1) * (G.nz + 1);
+  cudaEvent_t e0 = ctx->ev[4], e1 = ctx->ev[5], e2 = ctx->ev[6], e3 = ctx->ev[7];
+  cudaEventRecord(e0, s);
+  SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->h_fluid, a->fluid, cells * 4, cudaMemcpyHostToDevice, s));
+  SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->h_fluid_active, a->fluid_active, cells, cudaMemcpyHostToDevice, s));
+  if (a->solid) {
+    SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->h_solid, a->solid, nodes * 4, cudaMemcpyHostToDevice, s));
+    SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->h_solid_active, a->solid_active, nodes, cudaMemcpyHostToDevice, s));
+  }
+  size_t nf[3];
+  for (int d = 0; d < 3; ++d) {
+    nf[d] = (size_t)(G.nx + (d == 0)) * (G.ny + (d == 1)) * (G.nz + (d == 2));
+    SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->h_vel[d], a->velocity[d], nf[d] * 4, cudaMemcpyHostToDevice, s));
+    SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->h_vact[d], a->velocity_active[d], nf[d], cudaMemcpyHostToDevice, s));
+    if (svel[d])
+      SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->h_svel[d], a->solid_velocity[d], nf[d] * 4, cudaMemcpyHostToDevice, s));
+  }
+  cudaEventRecord(e1, s);
+  shkz_b200_project_args da = *a;
+  da.fluid = ctx->h_fluid;
+  da.fluid_active = ctx->h_fluid_active;
+  da.solid = a->solid ? ctx->h_solid : nullptr;
+  da.solid_active = a->solid ? ctx->h_solid_active : nullptr;
+  for (int d = 0; d < 3; ++d) {
+    da.velocity[d] = ctx->h_vel[d];
+    da.velocity_active[d] = ctx->h_vact[d];
+    da.solid_velocity[d] = svel[d] ? ctx->h_svel[d] : nullptr;
+  }
+  da.pressure = ctx->h_pressure;
+  da.pressure_active = ctx->h_pact;
+  rc = project_device(ctx, &da, res);
+  if (rc && rc != SHKZ_B200_ERR_NAN && rc != SHKZ_B200_ERR_TIMEOUT) return res->status = rc;
+  cudaEventRecord(e2, s);
+  for (int d = 0; d < 3; ++d) {
+    SHKZ_CUDA_TRY(cudaMemcpyAsync(a->velocity[d], ctx->h_vel[d], nf[d] * 4, cudaMemcpyDeviceToHost, s));
+    SHKZ_CUDA_TRY(cudaMemcpyAsync(a->velocity_active[d], ctx->h_vact[d], nf[d], cudaMemcpyDeviceToHost, s));
+  }
+  if (a->pressure) SHKZ_CUDA_TRY(cudaMemcpyAsync(a->pressure, ctx->h_pressure, cells * 4, cudaMemcpyDeviceToHost, s));
+  if (a->pressure_active)
+    SHKZ_CUDA_TRY(cudaMemcpyAsync(a->pressure_active, ctx->h_pact, cells, cudaMemcpyDeviceToHost, s));
+  cudaEventRecord(e3, s);
+  SHKZ_CUDA_TRY(cudaStreamSynchronize(s));
+  res->ms_h2d = ms_between(e0, e1);
+  res->ms_d2h = ms_between(e2, e3);
+  res->ms_total = ms_between(e0, e3);
+  res->status = rc;
+  return rc;
+}
+
+// --------------------------------------------------------------------------
+// inspection helpers (dense <-> pool)
+
+__global__ void k_pool_to_dense_f32(Geometry G, const int *tile_state, const float *pool, float *dense) {
+  const size_t n = (size_t)G.nx * G.ny * G.nz;
+  for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(c % G.nx), j = (int)((c / G.nx) % G.ny), k = (int)(c / ((size_t)G.nx * G.ny));
+    const long long t = (long long)(i >> 3) + (long long)G.bx * ((long long)(j >> 3) + (long long)G.by * (k >> 3));
+    const int pt = tile_state[t];
+    dense[c] = pt >= 0 ? pool[(size_t)pt * SHKZ_TC + (i & 7) + 8 * (j & 7) + 64 * (k & 7)] : 0.0f;
+  }
+}
+__global__ void k_pool_to_dense_f64(Geometry G, const int *tile_state, const double *pool, double *dense) {
+  const size_t n = (size_t)G.nx * G.ny * G.nz;
+  for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(c % G.nx), j = (int)((c / G.nx) % G.ny), k = (int)(c / ((size_t)G.nx * G.ny));
+    const long long t = (long long)(i >> 3) + (long long)G.bx * ((long long)(j >> 3) + (long long)G.by * (k >> 3));
+    const int pt = tile_state[t];
+    dense[c] = pt >= 0 ? pool[(size_t)pt * SHKZ_TC + (i & 7) + 8 * (j & 7) + 64 * (k & 7)] : 0.0;
+  }
+}
+__global__ void k_dense_to_pool_f32(Geometry G, const int *pool_tile, int K, const float *dense, float *pool) {
+  const size_t n = (size_t)K * SHKZ_TC;
+  for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < n; o += (size_t)gridDim.x * blockDim.x) {
+    const int pt = (int)(o >> 9), c = (int)(o & 511);
+    const long long t = pool_tile[pt];
+    const int i = (int)(t % G.bx) * 8 + (c & 7), j = (int)((t / G.bx) % G.by) * 8 + ((c >> 3) & 7),
+              k = (int)(t / ((long long)G.bx * G.by)) * 8 + (c >> 6);
+    float v = 0.0f;
+    if (i < G.nx && j < G.ny && k < G.nz) v = dense[(size_t)i + (size_t)G.nx * ((size_t)j + (size_t)G.ny * k)];
+    pool[o] = v;
+  }
+}
+
+extern "C" int shkz_b200_inspect(shkz_b200_ctx *ctx, int what, void *host_out, size_t bytes) {
+  if (!ctx || !host_out) return SHKZ_B200_ERR_ARG;
+  if (!ctx->has_system) return SHKZ_B200_ERR_STATE;
+  const Geometry &G = ctx->G;
+  const size_t cells = (size_t)G.nx * G.ny * G.nz;
+  const bool f64 = (what >= 5);
+  if (bytes < cells * (f64 ? 8 : 4)) return SHKZ_B200_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  void *dense = nullptr;
+  SHKZ_CUDA_TRY(cudaMalloc(&dense, cells * (f64 ? 8 : 4)));
+  const float *src32 = nullptr;
+  const double *src64 = nullptr;
+  switch (what) {
+    case 0: src32 = ctx->diag; break;
+    case 1: src32 = ctx->offx; break;
+    case 2: src32 = ctx->offy; break;
+    case 3: src32 = ctx->offz; break;
+    case 4: src32 = ctx->d32; break;
+    case 5: src64 = ctx->rhs64; break;
+    case 6: src64 = ctx->x64; break;
+    case 7: src64 = ctx->xref64; break;
+    default: cudaFree(dense); return SHKZ_B200_ERR_ARG;
+  }
+  count_launches(1);
+  if (src32) k_pool_to_dense_f32<<<148 * 8, 256, 0, s>>>(G, ctx->tile_state, src32, (float *)dense);
+  else k_pool_to_dense_f64<<<148 * 8, 256, 0, s>>>(G, ctx->tile_state, src64, (double *)dense);
+  cudaError_t e = cudaMemcpyAsync(host_out, dense, cells * (f64 ? 8 : 4), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFree(dense);
+  if (e != cudaSuccess) {
+    shkz_set_cuda_error(e, "inspect", __FILE__, __LINE__);
+    return SHKZ_B200_ERR_CUDA;
+  }
+  return 0;
+}
+
+static int dense_roundtrip(shkz_b200_ctx *ctx, const float *in_cells, float *out_cells, int op) {
+  if (!ctx || !in_cells || !out_cells) return SHKZ_B200_ERR_ARG;
+  if (!ctx->has_system) return SHKZ_B200_ERR_STATE;
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  const Geometry &G = ctx->G;
+  const size_t cells = (size_t)G.nx * G.ny * G.nz;
+  const int n = ctx->K * SHKZ_TC;
+  float *dense = nullptr;
+  SHKZ_CUDA_TRY(cudaMalloc(&dense, cells * 4));
+  cudaMemcpyAsync(dense, in_cells, cells * 4, cudaMemcpyHostToDevice, s);
+  if (ctx->K > 0) {
+    count_launches(1);
+    k_dense_to_pool_f32<<<148 * 8, 256, 0, s>>>(G, ctx->pool_tile, ctx->K, dense, ctx->r);
+    const PoolSystem S = pool_system(ctx);
+    if (op == 0) {
+      launch_spmv(S, ctx->r, ctx->z, ctx->partials, ctx->counter, nullptr, 1, s);
+    } else if (ctx->cfg.preconditioner == SHKZ_B200_PRECOND_MIC0 || ctx->cfg.preconditioner == SHKZ_B200_PRECOND_LEARNED) {
+      launch_mic_apply(S, ctx->d32, ctx->r, ctx->t, ctx->z, nullptr, ctx->wflags + ctx->cap_pool,
+                       ctx->wflags + 2 * ctx->cap_pool, wsync(ctx, 1), wsync(ctx, 2), nullptr, s);
+    } else {
+      cudaMemcpyAsync(ctx->z, ctx->r, sizeof(float) * n, cudaMemcpyDeviceToDevice, s);
+    }
+    count_launches(1);
+    k_pool_to_dense_f32<<<148 * 8, 256, 0, s>>>(G, ctx->tile_state, ctx->z, dense);
+  } else {
+    cudaMemsetAsync(dense, 0, cells * 4, s);
+  }
+  cudaError_t e = cudaMemcpyAsync(out_cells, dense, cells * 4, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFree(dense);
+  if (e != cudaSuccess) {
+    shkz_set_cuda_error(e, "roundtrip", __FILE__, __LINE__);
+    return SHKZ_B200_ERR_CUDA;
+  }
+  if (wave_errors(ctx)) return SHKZ_B200_ERR_TIMEOUT;
+  return 0;
+}
+
+extern "C" int shkz_b200_apply_preconditioner(shkz_b200_ctx *ctx, const float *r_cells, float *z_cells) {
+  return dense_roundtrip(ctx, r_cells, z_cells, 1);
+}
+extern "C" int shkz_b200_apply_matrix(shkz_b200_ctx *ctx, const float *x_cells, float *y_cells) {
+  return dense_roundtrip(ctx, x_cells, y_cells, 0);
+}
+
+// --------------------------------------------------------------------------
+// Generic CSR path for LinSolver=: the shipped pcg_solver algorithm
+// (PCGSolver::solve, local/include/pcgsolver/pcg_solver.h:246-295) whose
+// preconditioner result is discarded (:379-384), i.e. CG in FP64 with
+// x0 = 0 and the stopping rule ||r||inf <= Residual * ||b||inf.
+
+__global__ void k_csr_spmv64(int n, const int *__restrict__ indptr, const int *__restrict__ indices,
+                             const double *__restrict__ data, const double *__restrict__ x, double *__restrict__ y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int p = indptr[i]; p < indptr[i + 1]; ++p) s += data[p] * x[indices[p]];
+    y[i] = s;
+  }
+}
+
+extern "C" int shkz_b200_solve_csr(shkz_b200_ctx *ctx, long long n, const long long *indptr,
+                                   const long long *indices, const double *data, const double *b, double *x,
+                                   shkz_b200_result *res) {
+  if (!ctx || !indptr || !indices || !data || !b || !x || !res || n < 0) return SHKZ_B200_ERR_ARG;
+  std::memset(res, 0, sizeof(*res));
+  if (n == 0) return 0;
+  const long long nnz = indptr[n];
+  if (n > INT32_MAX || nnz > INT32_MAX) return res->status = SHKZ_B200_ERR_LIMIT;
+  if (ctx->cfg.preconditioner != SHKZ_B200_PRECOND_NONE) return res->status = SHKZ_B200_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  std::vector<int> hp((size_t)n + 1), hi((size_t)nnz);
+  for (long long i = 0; i <= n; ++i) hp[i] = (int)indptr[i];
+  for (long long i = 0; i < nnz; ++i) hi[i] = (int)indices[i];
+  int *dp = nullptr, *di = nullptr;
+  double *dd = nullptr, *vb = nullptr;
+  auto cleanup = [&]() {
+    if (dp) cudaFree(dp);
+    if (di) cudaFree(di);
+    if (dd) cudaFree(dd);
+    if (vb) cudaFree(vb);
+  };
+  // vectors: r, x, s(p), z(q) and reduction scratch
+  if (cudaMalloc(&dp, sizeof(int) * (n + 1)) != cudaSuccess || cudaMalloc(&di, sizeof(int) * (nnz ? nnz : 1)) != cudaSuccess ||
+      cudaMalloc(&dd, sizeof(double) * (nnz ? nnz : 1)) != cudaSuccess ||
+      cudaMalloc(&vb, sizeof(double) * (4 * (size_t)n + 3 * 8192 + 8)) != cudaSuccess) {
+    cleanup();
+    return res->status = SHKZ_B200_ERR_NOMEM;
+  }
+  double *r = vb, *xv = vb + n, *p = vb + 2 * n, *q = vb + 3 * n, *part = vb + 4 * n, *out = part + 3 * 8192;
+  unsigned *cnt = ctx->counter + 4;
+  cudaMemcpyAsync(dp, hp.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(di, hi.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(dd, data, sizeof(double) * nnz, cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(r, b, sizeof(double) * n, cudaMemcpyHostToDevice, s);
+  cudaMemsetAsync(xv, 0, sizeof(double) * n, s);
+  double h[3];
+  auto dots = [&](const double *a, const double *bb) -> bool {
+    launch_dots64((int)n, a, bb, nullptr, nullptr, part, cnt, out, s);
+    return cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+           cudaStreamSynchronize(s) == cudaSuccess;
+  };
+  int rc = 0, it = 0;
+  if (!dots(r, r)) { cleanup(); return res->status = SHKZ_B200_ERR_CUDA; }
+  const double r0 = h[2];
+  double rmax = r0;
+  if (r0 == 0.0) {
+    res->iterations = 0;
+    res->reresid = 0.0;
+  } else {
+    const double tol = ctx->cfg.residual * r0;
+    double rho = h[0];
+    cudaMemcpyAsync(p, r, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
+    const int grid = (int)std::min<long long>((n + 255) / 256, 148 * 16);
+    for (it = 0; it < ctx->cfg.max_iterations; ++it) {
+      count_launches(1);
+      k_csr_spmv64<<<grid, 256, 0, s>>>((int)n, dp, di, dd, p, q);
+      if (!dots(p, q)) { rc = SHKZ_B200_ERR_CUDA; break; }
+      const double alpha = rho / h[0];
+      launch_axpy2_64((int)n, alpha, p, xv, q, r, s);
+      if (!dots(r, r)) { rc = SHKZ_B200_ERR_CUDA; break; }
+      rmax = h[2];
+      if (!(rmax == rmax)) { rc = SHKZ_B200_ERR_NAN; break; }
+      if (rmax <= tol) { ++it; break; }
+      const double rho_new = h[0];
+      launch_xpby64((int)n, r, rho_new / rho, p, s);
+      rho = rho_new;
+    }
+    res->iterations = it;
+    res->reresid = rmax / r0;
+  }
+  if (cudaMemcpyAsync(x, xv, sizeof(double) * n, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    rc = SHKZ_B200_ERR_CUDA;
+  cleanup();
+  res->unknowns = n;
+  res->status = rc;
+  return rc;
+}
+
+extern "C" int shkz_b200_time_kernel(shkz_b200_ctx *ctx, int which, int reps, double *ms, long long *cells_out) {
+  if (!ctx || !ms || reps <= 0) return SHKZ_B200_ERR_ARG;
+  if (!ctx->has_system) return SHKZ_B200_ERR_STATE;
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  const PoolSystem S = pool_system(ctx);
+  const int n = ctx->K * SHKZ_TC;
+  SolverState init{};
+  init.rho = 1.0;
+  init.alpha = 1e-30;  // keeps x and r unchanged to rounding while timing the update
+  init.beta = 0.0;
+  init.tol_abs = -1.0;
+  SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->st_scratch, &init, sizeof(init), cudaMemcpyHostToDevice, s));
+  auto launch = [&]() {
+    switch (which) {
+      case 0: launch_spmv(S, ctx->p, ctx->q, ctx->partials, ctx->counter, ctx->st_scratch, 0, s); break;
+      case 1:
+      case 2: {
+        // forward and backward are timed as a pair; the split uses two event pairs below
+        launch_mic_apply(S, ctx->d32, ctx->r, ctx->t, ctx->z, ctx->partials, ctx->wflags + ctx->cap_pool,
+                         ctx->wflags + 2 * ctx->cap_pool, wsync(ctx, 1), wsync(ctx, 2), nullptr, s);
+        break;
+      }
+      case 3: launch_update_xr(n, ctx->p, ctx->q, ctx->x, ctx->r, ctx->partials, ctx->counter + 1, ctx->st_scratch,
+                               1 << 30, s); break;
+      case 4: launch_update_p(n, ctx->z, ctx->p, ctx->st_scratch, s); break;
+      case 5: launch_label(ctx->last_in, ctx->flags, ctx->unk, ctx->tile_count, s); break;
+      case 6: {
+        CoeffOutputs co{ctx->diag, ctx->offx, ctx->offy, ctx->offz, ctx->diag64, ctx->offx64, ctx->offy64,
+                        ctx->offz64, ctx->rhs64};
+        launch_coeff(ctx->last_in, ctx->flags, ctx->pool_tile, ctx->K, ctx->unk, co, s);
+        break;
+      }
+      case 7: launch_mic_factor(S, ctx->colsum, ctx->cfg.mic_omega, ctx->cfg.mic_min_diag_ratio, ctx->dmic64,
+                                ctx->d32, ctx->wflags, wsync(ctx, 0), s); break;
+      default: break;
+    }
+  };
+  if (which < 0 || which > 7) return SHKZ_B200_ERR_ARG;
+  launch();  // warm-up
+  SHKZ_CUDA_TRY(cudaStreamSynchronize(s));
+  double total = 0.0;
+  if (which == 1 || which == 2) {
+    // time the two sweeps separately: forward then backward, each bracketed
+    for (int i = 0; i < reps; ++i) {
+      cudaEventRecord(ctx->ev[4], s);
+      launch_mic_apply(S, ctx->d32, ctx->r, ctx->t, ctx->z, ctx->partials, ctx->wflags + ctx->cap_pool,
+                       ctx->wflags + 2 * ctx->cap_pool, wsync(ctx, 1), wsync(ctx, 2), nullptr, s);
+      cudaEventRecord(ctx->ev[5], s);
+      SHKZ_CUDA_TRY(cudaEventSynchronize(ctx->ev[5]));
+      total += ms_between(ctx->ev[4], ctx->ev[5]);
+    }
+    *ms = total / reps;
+  } else {
+    cudaEventRecord(ctx->ev[4], s);
+    for (int i = 0; i < reps; ++i) launch();
+    cudaEventRecord(ctx->ev[5], s);
+    SHKZ_CUDA_TRY(cudaEventSynchronize(ctx->ev[5]));
+    *ms = ms_between(ctx->ev[4], ctx->ev[5]) / reps;
+  }
+  SHKZ_CUDA_TRY(cudaGetLastError());
+  if (cells_out) *cells_out = (which == 5) ? (long long)ctx->G.nx * ctx->G.ny * ctx->G.nz : (long long)n;
+  if (wave_errors(ctx)) return SHKZ_B200_ERR_TIMEOUT;
+  return 0;
+}

@@ -1,0 +1,44 @@
+// Host-side launch interfaces shared by the CUDA translation units.
+#pragma once
+#include "common.cuh"
+
+namespace shkz {
+
+struct AssemblyInputs {
+  Geometry G;
+  const float *fluid;
+  const uint8_t *fluid_active;
+  const float *solid;          // may be null
+  const uint8_t *solid_active; // may be null
+  const float *vel[3];
+  const float *svel[3];        // each may be null
+  double dx, dt;
+  double eps_solid, eps_fluid;
+  int second_order_fluid, second_order_solid;
+};
+
+struct CoeffOutputs {
+  float *diag, *offx, *offy, *offz;
+  double *diag64, *offx64, *offy64, *offz64;   // may be null
+  double *rhs64;
+};
+
+// Pool-resident system in 8^3 tiles.
+struct PoolSystem {
+  int K;                 // tiles in the pool
+  const int *nbr;        // [K][6] pool index of neighbour tiles or -1
+  const int *sched;      // [K] pool indices ordered by wavefront level
+  const float *diag, *offx, *offy, *offz;
+  const double *diag64, *offx64, *offy64, *offz64;
+};
+
+// assemble.cu
+void launch_label(const AssemblyInputs &in, int *flags, uint8_t *unk, int *tile_count, cudaStream_t s);
+void launch_coeff(const AssemblyInputs &in, const int *flags, const int *pool_tile, int K, const uint8_t *unk,
+                  const CoeffOutputs &out, cudaStream_t s);
+void launch_velocity_update(const AssemblyInputs &in, const int *flags, const int *tile_state,
+                            const float *pressure_pool, float *const vel[3], uint8_t *const vact[3], cudaStream_t s);
+void launch_scatter_pressure(const Geometry &G, const int *tile_state, const float *pressure_pool, const uint8_t *unk,
+                             float *pressure, uint8_t *pressure_active, cudaStream_t s);
+
+}  // namespace shkz

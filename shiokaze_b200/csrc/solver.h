@@ -1,0 +1,41 @@
+// Launch interfaces of the PCG / MIC(0) kernels (solver.cu).
+#pragma once
+#include "common.cuh"
+#include "kernels.h"
+
+namespace shkz {
+
+// Number of tiles holding unknowns (synchronises the stream), then the pool itself.
+int pool_count(const Geometry &G, const int *tile_count, int *scratch_bsum, int *d_total, cudaStream_t s);
+void pool_assign(const Geometry &G, const int *tile_count, int K, const int *scratch_bsum, int *tile_state,
+                 int *pool_tile, int *nbr, int *level_count, int *sched, cudaStream_t s);
+size_t wave_sync_bytes();
+int spmv_grid(int K);
+void launch_spmv(const PoolSystem &S, const float *p, float *q, double *partials, unsigned *counter, SolverState *st,
+                 int mode, cudaStream_t s);
+void launch_update_xr(int n, const float *p, const float *q, float *x, float *r, double *partials, unsigned *counter,
+                      SolverState *st, int max_iterations, cudaStream_t s);
+void launch_finish_rho(const double *partials, int n, SolverState *st, int init, cudaStream_t s);
+void launch_finish_rho_r2(SolverState *st, int init, cudaStream_t s);
+void launch_update_p(int n, const float *z, float *p, const SolverState *st, cudaStream_t s);
+void launch_mic_factor(const PoolSystem &S, double *colsum, double omega, double min_ratio, double *d64, float *d32,
+                       int *flags, void *ws, cudaStream_t s);
+void launch_mic_apply(const PoolSystem &S, const float *d32, const float *r, float *t, float *z, double *partials,
+                      int *flags_f, int *flags_b, void *ws_f, void *ws_b, const SolverState *st, cudaStream_t s);
+void launch_residual64(const PoolSystem &S, const double *b, const double *x, double *r, double *partials,
+                       unsigned *counter, double *out4, cudaStream_t s);
+void launch_inner_init(int n, const double *r64, double inv_scale, float *r32, float *x32, cudaStream_t s);
+void launch_accumulate(int n, const float *x32, double scale, double *x64, cudaStream_t s);
+void launch_to_float(int n, const double *a, float *b, cudaStream_t s);
+void launch_inner_setup(int n, const float *r, double *partials, unsigned *counter, SolverState *st, double tol,
+                        cudaStream_t s);
+
+void launch_apply64(const PoolSystem &S, const double *x, double *y, cudaStream_t s);
+void launch_dots64(int n, const double *a, const double *b, const double *c, const double *d, double *partials,
+                   unsigned *counter, double *out, cudaStream_t s);
+void launch_axpy2_64(int n, double alpha, const double *x, double *y, const double *q, double *r, cudaStream_t s);
+void launch_xpby64(int n, const double *x, double beta, double *y, cudaStream_t s);
+void launch_scale_f64_f32(int n, const double *a, double sc, float *b, cudaStream_t s);
+void launch_scale_f32_f64(int n, const float *a, double sc, double *b, cudaStream_t s);
+
+}  // namespace shkz

@@ -1,0 +1,165 @@
+"""ctypes binding of the C ABI in ``include/shkz_b200.h``.
+
+Loads the in-tree ``libshkz_b200.so``; importing this module on a machine
+without the built library or without a CUDA device raises instead of falling
+back to anything else.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libshkz_b200.so")
+
+PRECOND_NONE = 0
+PRECOND_MIC0 = 1
+PRECOND_LEARNED = 2
+
+ERRORS = {
+    0: "ok", -1: "invalid argument", -2: "CUDA runtime error", -3: "device allocation failed",
+    -4: "a bounded device wait gave up", -5: "NaN in the system or the iterates",
+    -6: "no usable sm_100 device", -7: "invalid call order", -8: "size beyond a documented limit",
+}
+
+
+class Config(ctypes.Structure):
+    _fields_ = [
+        ("residual", ctypes.c_double),
+        ("max_iterations", ctypes.c_int),
+        ("preconditioner", ctypes.c_int),
+        ("mic_omega", ctypes.c_double),
+        ("mic_min_diag_ratio", ctypes.c_double),
+        ("eps_fluid", ctypes.c_double),
+        ("eps_solid", ctypes.c_double),
+        ("second_order_fluid", ctypes.c_int),
+        ("second_order_solid", ctypes.c_int),
+        ("refine", ctypes.c_int),
+        ("fp64_reference", ctypes.c_int),
+        ("fp64_tol", ctypes.c_double),
+        ("check_interval", ctypes.c_int),
+        ("stall_window", ctypes.c_int),
+        ("device", ctypes.c_int),
+        ("reserved", ctypes.c_int * 8),
+    ]
+
+
+class ProjectArgs(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("dx", ctypes.c_double), ("dt", ctypes.c_double),
+        ("fluid", ctypes.c_void_p), ("fluid_active", ctypes.c_void_p),
+        ("solid", ctypes.c_void_p), ("solid_active", ctypes.c_void_p),
+        ("velocity", ctypes.c_void_p * 3), ("velocity_active", ctypes.c_void_p * 3),
+        ("solid_velocity", ctypes.c_void_p * 3),
+        ("pressure", ctypes.c_void_p), ("pressure_active", ctypes.c_void_p),
+    ]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [
+        ("status", ctypes.c_int), ("iterations", ctypes.c_int), ("outer_steps", ctypes.c_int),
+        ("fallbacks", ctypes.c_int), ("unknowns", ctypes.c_longlong), ("tiles", ctypes.c_longlong),
+        ("reresid", ctypes.c_double), ("reresid_l2", ctypes.c_double), ("err_fp64_inf", ctypes.c_double),
+        ("fp64_reresid", ctypes.c_double), ("ms_assemble", ctypes.c_double), ("ms_solve", ctypes.c_double),
+        ("ms_update", ctypes.c_double), ("ms_total", ctypes.c_double), ("ms_h2d", ctypes.c_double),
+        ("ms_d2h", ctypes.c_double), ("kernel_launches", ctypes.c_longlong), ("reserved", ctypes.c_double * 7),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+EXPORTS = [
+    "shkz_b200_default_config", "shkz_b200_create", "shkz_b200_destroy", "shkz_b200_set_config",
+    "shkz_b200_errstr", "shkz_b200_last_error", "shkz_b200_project_host", "shkz_b200_project_device",
+    "shkz_b200_stream", "shkz_b200_solve_csr", "shkz_b200_inspect", "shkz_b200_apply_preconditioner",
+    "shkz_b200_apply_matrix", "shkz_b200_time_kernel",
+]
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load the CUDA library (raises OSError if it is missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise OSError(f"{path} is not built; run `python -m shiokaze_b200.build`")
+    L = ctypes.CDLL(path)
+    P = ctypes.c_void_p
+    L.shkz_b200_default_config.argtypes = [ctypes.POINTER(Config)]
+    L.shkz_b200_create.argtypes = [ctypes.POINTER(P), ctypes.POINTER(Config)]
+    L.shkz_b200_create.restype = ctypes.c_int
+    L.shkz_b200_destroy.argtypes = [P]
+    L.shkz_b200_set_config.argtypes = [P, ctypes.POINTER(Config)]
+    L.shkz_b200_errstr.argtypes = [ctypes.c_int]
+    L.shkz_b200_errstr.restype = ctypes.c_char_p
+    L.shkz_b200_last_error.argtypes = [P]
+    L.shkz_b200_last_error.restype = ctypes.c_char_p
+    L.shkz_b200_project_host.argtypes = [P, ctypes.POINTER(ProjectArgs), ctypes.POINTER(Result)]
+    L.shkz_b200_project_device.argtypes = [P, ctypes.POINTER(ProjectArgs), ctypes.POINTER(Result)]
+    L.shkz_b200_stream.argtypes = [P]
+    L.shkz_b200_stream.restype = P
+    L.shkz_b200_solve_csr.argtypes = [P, ctypes.c_longlong, P, P, P, P, P, ctypes.POINTER(Result)]
+    L.shkz_b200_inspect.argtypes = [P, ctypes.c_int, P, ctypes.c_size_t]
+    L.shkz_b200_apply_preconditioner.argtypes = [P, P, P]
+    L.shkz_b200_apply_matrix.argtypes = [P, P, P]
+    L.shkz_b200_time_kernel.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                        ctypes.POINTER(ctypes.c_longlong)]
+    _lib = L
+    return L
+
+
+def default_config() -> Config:
+    c = Config()
+    load().shkz_b200_default_config(ctypes.byref(c))
+    return c
+
+
+class ShkzError(RuntimeError):
+    def __init__(self, code: int, where: str, detail: str = ""):
+        self.code = code
+        super().__init__(f"{where}: {ERRORS.get(code, code)} ({code}) {detail}".strip())
+
+
+class Context:
+    """Owns one device context (``shkz_b200_create`` / ``shkz_b200_destroy``)."""
+
+    def __init__(self, config: Config | None = None):
+        L = load()
+        self.config = config if config is not None else default_config()
+        h = ctypes.c_void_p()
+        rc = L.shkz_b200_create(ctypes.byref(h), ctypes.byref(self.config))
+        if rc != 0:
+            raise ShkzError(rc, "shkz_b200_create")
+        self.handle = h
+
+    def set_config(self, config: Config):
+        self.config = config
+        rc = load().shkz_b200_set_config(self.handle, ctypes.byref(config))
+        if rc != 0:
+            raise ShkzError(rc, "shkz_b200_set_config")
+
+    def close(self):
+        if getattr(self, "handle", None):
+            load().shkz_b200_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def last_error(self) -> str:
+        return load().shkz_b200_last_error(self.handle).decode()
+
+    def check(self, rc: int, where: str):
+        if rc != 0:
+            raise ShkzError(rc, where, self.last_error())
+
+    @property
+    def stream(self) -> int:
+        return load().shkz_b200_stream(self.handle)
