@@ -63,7 +63,8 @@ def read_system(path: str) -> dict:
 
 def run_reference(scene, variant: str = "float", mode: str = "mic0", tol: Optional[float] = None,
                   threads: Optional[int] = None, tile_size: int = 8, dump_system: bool = True,
-                  repeat: int = 1, extra: Optional[dict] = None, linsolver: str = "refmic0") -> RefResult:
+                  repeat: int = 1, extra: Optional[dict] = None, linsolver: str = "refmic0",
+                  extra_libpath: Optional[list] = None) -> RefResult:
     exe = os.path.join(REF_DIR, variant, "shkz_ref_harness")
     if not os.path.exists(exe):
         raise FileNotFoundError(exe)
@@ -78,7 +79,8 @@ def run_reference(scene, variant: str = "float", mode: str = "mic0", tol: Option
         for k, v in (extra or {}).items():
             args.append(f"{k}={v}")
         env = dict(os.environ)
-        env["LD_LIBRARY_PATH"] = os.path.join(REF_DIR, variant) + ":" + env.get("LD_LIBRARY_PATH", "")
+        env["LD_LIBRARY_PATH"] = ":".join(list(extra_libpath or []) + [os.path.join(REF_DIR, variant),
+                                                                          env.get("LD_LIBRARY_PATH", "")])
         dump = os.path.join(td, "dump")
         env["SHKZ_REF_DUMP"] = dump if dump_system else ""
         proc = subprocess.run(args, cwd=td, env=env, capture_output=True, text=True)

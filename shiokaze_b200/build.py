@@ -60,5 +60,34 @@ def build(verbose: bool = False, extra=None) -> str:
     return LIB
 
 
+PLUGINS = {"libshiokaze_macpressuresolver3_b200.so": "macpressuresolver3_b200.cpp"}
+
+
+def build_plugins(reference_root: str, verbose: bool = False) -> list:
+    """Build the Shiokaze module(s) that wrap the C ABI. They compile against
+    the reference's public headers (``<reference_root>/include`` and
+    ``local/include``) with the reference's build defines, and link
+    ``libshkz_b200.so`` from this directory."""
+    inc = os.path.join(reference_root, "include")
+    if not os.path.isdir(inc):
+        return []
+    lib = build(verbose=verbose)
+    out = []
+    for so, src in PLUGINS.items():
+        target = os.path.join(HERE, so)
+        source = os.path.join(HERE, "plugin", src)
+        if _stale(target, [source, lib, os.path.join(HERE, "..", "include", "shkz_b200.h")]):
+            cmd = ["g++", "-std=c++17", "-O3", "-fPIC", "-shared", "-w",
+                   '-DSHKZ_SUFFIX=""', "-DSHKZ_RELEASE=1", f"-DNUM_THREAD={os.cpu_count() or 4}",
+                   "-I" + inc, "-I" + os.path.join(reference_root, "local", "include"),
+                   "-I" + os.path.join(HERE, "..", "include"), source, "-o", target,
+                   "-L" + HERE, "-lshkz_b200", "-Wl,-rpath,$ORIGIN"]
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            subprocess.check_call(cmd)
+        out.append(target)
+    return out
+
+
 if __name__ == "__main__":
     build(verbose=True, extra=sys.argv[1:])

@@ -58,7 +58,8 @@ struct shkz_b200_ctx {
   double *partials = nullptr, *out4 = nullptr;
   unsigned *counter = nullptr;
   SolverState *st = nullptr;
-  int *wflags = nullptr;  // [3][cap_pool]
+  int *wflags = nullptr;  // factor wavefront flags [cap_pool]
+  unsigned long long *faces_f = nullptr, *faces_b = nullptr;  // [cap_pool][3][64] epoch-tagged sweep faces
   void *ws = nullptr;     // 3 WaveSync
   // last projection
   Geometry G{};
@@ -200,8 +201,12 @@ static int ensure_pool(shkz_b200_ctx *ctx, int K) {
   GROW(p64, n); GROW(q64, n); GROW(z64, n);
   GROW(x, n); GROW(r, n); GROW(p, n); GROW(q, n); GROW(z, n); GROW(t, n); GROW(p32, n);
   GROW(partials, (size_t)cap + 4 * 8192);
-  GROW(wflags, (size_t)3 * cap);
-  SHKZ_CUDA_TRY(cudaMemsetAsync(ctx->wflags, 0, sizeof(int) * 3 * (size_t)cap, ctx->stream));
+  GROW(wflags, (size_t)cap);
+  GROW(faces_f, (size_t)cap * 3 * 64);
+  GROW(faces_b, (size_t)cap * 3 * 64);
+  SHKZ_CUDA_TRY(cudaMemsetAsync(ctx->wflags, 0, sizeof(int) * (size_t)cap, ctx->stream));
+  SHKZ_CUDA_TRY(cudaMemsetAsync(ctx->faces_f, 0, sizeof(unsigned long long) * (size_t)cap * 3 * 64, ctx->stream));
+  SHKZ_CUDA_TRY(cudaMemsetAsync(ctx->faces_b, 0, sizeof(unsigned long long) * (size_t)cap * 3 * 64, ctx->stream));
   if (ctx->ws) {
     // flags were reset: restart the epochs
     SHKZ_CUDA_TRY(cudaMemsetAsync(ctx->ws, 0, 3 * wave_sync_bytes(), ctx->stream));
@@ -265,7 +270,7 @@ extern "C" void shkz_b200_destroy(shkz_b200_ctx *ctx) {
                   ctx->offz64, ctx->rhs64, ctx->colsum, ctx->dmic64, ctx->x64, ctx->r64, ctx->xref64, ctx->p64, ctx->q64,
                   ctx->z64, ctx->x, ctx->r,
                   ctx->p, ctx->q, ctx->z, ctx->t, ctx->p32, ctx->partials, ctx->out4, ctx->counter, ctx->st,
-                  ctx->wflags, ctx->ws, ctx->st_scratch};
+                  ctx->wflags, ctx->faces_f, ctx->faces_b, ctx->ws, ctx->st_scratch};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (ctx->model) learned_free(ctx->model);
@@ -315,54 +320,32 @@ static int wave_errors(shkz_b200_ctx *ctx) {
 }
 
 // --------------------------------------------------------------------------
-// Inner FP32 PCG on (A32, r, x): the reference loop, batched.
-// Returns iterations; *done_code gets the solver's done value.
-static int inner_pcg(shkz_b200_ctx *ctx, double tol, int max_it, int precond, int *done_code) {
-  cudaStream_t s = ctx->stream;
-  const PoolSystem S = pool_system(ctx);
-  const int n = ctx->K * SHKZ_TC;
-  launch_inner_setup(n, ctx->r, ctx->partials, ctx->counter, ctx->st, tol, s);
-  // z = M^-1 r, rho = z.r, p = z
+// FP32 PCG with FP64 reductions and reliable updates.
+//
+// One PCG recurrence (the reference loop, pcg_solver.h:246-295) runs on FP32
+// vectors scaled by 1/||b||inf. The solution is accumulated in FP64: each time
+// the recursive residual has dropped by `kReliableDrop` since the last update,
+// and whenever it meets the tolerance, the FP32 increment is added to x64, the
+// true residual b - A x64 is recomputed in FP64 and replaces the recursive one,
+// and the search direction is kept. The stopping test is always decided on the
+// true FP64 residual, so FP32 rounding never ends a solve early and the
+// iteration count stays that of the FP64 recurrence.
+
+static const double kReliableDrop = 0.1;
+
+// z = M^-1 r, rho_new, beta, p = z + beta p (or the identity-preconditioned variant)
+static void launch_iteration_tail(shkz_b200_ctx *ctx, const PoolSystem &S, int n, int precond, cudaStream_t s) {
   if (precond == SHKZ_B200_PRECOND_MIC0) {
-    launch_mic_apply(S, ctx->d32, ctx->r, ctx->t, ctx->z, ctx->partials, ctx->wflags + ctx->cap_pool,
-                     ctx->wflags + 2 * ctx->cap_pool, wsync(ctx, 1), wsync(ctx, 2), ctx->st, s);
-    launch_finish_rho(ctx->partials, ctx->K, ctx->st, 1, s);
-    cudaMemcpyAsync(ctx->p, ctx->z, sizeof(float) * n, cudaMemcpyDeviceToDevice, s);
+    launch_mic_apply(S, ctx->d32, ctx->r, ctx->t, ctx->z, ctx->partials, ctx->faces_f,
+                     ctx->faces_b, wsync(ctx, 1), wsync(ctx, 2), ctx->st, s);
+    launch_finish_rho(ctx->partials, ctx->K, ctx->st, 0, s);
+    launch_update_p(n, ctx->z, ctx->p, ctx->st, s);
   } else {
-    launch_finish_rho_r2(ctx->st, 1, s);
-    cudaMemcpyAsync(ctx->p, ctx->r, sizeof(float) * n, cudaMemcpyDeviceToDevice, s);
+    launch_finish_rho_r2(ctx->st, 0, s);
+    launch_update_p(n, ctx->r, ctx->p, ctx->st, s);
   }
-  const int batch = ctx->cfg.check_interval > 0 ? ctx->cfg.check_interval : 16;
-  SolverState hst;
-  int launched = 0;
-  for (;;) {
-    for (int b = 0; b < batch && launched < max_it; ++b, ++launched) {
-      launch_spmv(S, ctx->p, ctx->q, ctx->partials, ctx->counter, ctx->st, 0, s);
-      launch_update_xr(n, ctx->p, ctx->q, ctx->x, ctx->r, ctx->partials, ctx->counter + 1, ctx->st, max_it, s);
-      if (precond == SHKZ_B200_PRECOND_MIC0) {
-        launch_mic_apply(S, ctx->d32, ctx->r, ctx->t, ctx->z, ctx->partials, ctx->wflags + ctx->cap_pool,
-                         ctx->wflags + 2 * ctx->cap_pool, wsync(ctx, 1), wsync(ctx, 2), ctx->st, s);
-        launch_finish_rho(ctx->partials, ctx->K, ctx->st, 0, s);
-        launch_update_p(n, ctx->z, ctx->p, ctx->st, s);
-      } else {
-        launch_finish_rho_r2(ctx->st, 0, s);
-        launch_update_p(n, ctx->r, ctx->p, ctx->st, s);
-      }
-    }
-    if (cudaMemcpyAsync(&hst, ctx->st, sizeof(hst), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-        cudaStreamSynchronize(s) != cudaSuccess) {
-      shkz_set_cuda_error(cudaGetLastError(), "inner_pcg sync", __FILE__, __LINE__);
-      *done_code = -1;
-      return -1;
-    }
-    if (hst.done || launched >= max_it) break;
-  }
-  *done_code = hst.done;
-  if (hst.status == -5) *done_code = 3;
-  return hst.iter;
 }
 
-// FP64 refinement around the FP32 PCG. x64 holds the solution on return.
 static int solve_system(shkz_b200_ctx *ctx, double tol, int precond, shkz_b200_result *res) {
   cudaStream_t s = ctx->stream;
   const PoolSystem S = pool_system(ctx);
@@ -374,42 +357,78 @@ static int solve_system(shkz_b200_ctx *ctx, double tol, int precond, shkz_b200_r
   SHKZ_CUDA_TRY(cudaStreamSynchronize(s));
   const double bmax = h4[2], b2 = h4[3];
   double rmax = h4[0], r2 = h4[1];
-  int iterations = 0, outer = 0, rc = 0;
+  res->outer_steps = 0;
   if (bmax == 0.0) {
     res->iterations = 0;
     res->reresid = 0.0;
     res->reresid_l2 = 0.0;
-    res->outer_steps = 0;
     return 0;
   }
-  const int max_outer = ctx->cfg.refine ? 12 : 1;
-  while (outer < max_outer) {
-    const double scale = rmax;
-    // inner relative tolerance: the target itself on the first pass, then
-    // what is left to gain (bounded below by what FP32 iterates can reach)
-    double tol_inner = (outer == 0) ? tol : std::fmax(0.5 * tol * bmax / rmax, 2e-6);
-    if (tol_inner > 0.5) tol_inner = 0.5;
-    launch_inner_init(n, ctx->r64, 1.0 / scale, ctx->r, ctx->x, s);
-    int done = 0;
-    const int it = inner_pcg(ctx, tol_inner, ctx->cfg.max_iterations - iterations, precond, &done);
-    if (it < 0) return SHKZ_B200_ERR_CUDA;
-    iterations += it;
+  if (!(b2 == b2)) {
+    res->iterations = 0;
+    return SHKZ_B200_ERR_NAN;
+  }
+  const double scale = bmax;
+  const bool reliable = ctx->cfg.refine != 0;
+  launch_inner_init(n, ctx->r64, 1.0 / scale, ctx->r, ctx->x, s);
+  launch_inner_setup(n, ctx->r, ctx->partials, ctx->counter, ctx->st, tol, s);
+  launch_state_resume(ctx->st, reliable ? kReliableDrop : 0.0, s);
+  // z0 = M^-1 r0, rho0, p0 = z0
+  if (precond == SHKZ_B200_PRECOND_MIC0) {
+    launch_mic_apply(S, ctx->d32, ctx->r, ctx->t, ctx->z, ctx->partials, ctx->faces_f,
+                     ctx->faces_b, wsync(ctx, 1), wsync(ctx, 2), ctx->st, s);
+    launch_finish_rho(ctx->partials, ctx->K, ctx->st, 1, s);
+    SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->p, ctx->z, sizeof(float) * n, cudaMemcpyDeviceToDevice, s));
+  } else {
+    launch_finish_rho_r2(ctx->st, 1, s);
+    SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->p, ctx->r, sizeof(float) * n, cudaMemcpyDeviceToDevice, s));
+  }
+  const int max_it = ctx->cfg.max_iterations;
+  const int batch = ctx->cfg.check_interval > 0 ? ctx->cfg.check_interval : 16;
+  SolverState hst;
+  int rc = 0, updates = 0;
+  bool true_checked = false;
+  for (;;) {
+    for (int b = 0; b < batch; ++b) {
+      launch_spmv(S, ctx->p, ctx->q, ctx->partials, ctx->counter, ctx->st, 0, s);
+      launch_update_xr(n, ctx->p, ctx->q, ctx->x, ctx->r, ctx->partials, ctx->counter + 1, ctx->st, max_it, s);
+      launch_iteration_tail(ctx, S, n, precond, s);
+    }
+    SHKZ_CUDA_TRY(cudaMemcpyAsync(&hst, ctx->st, sizeof(hst), cudaMemcpyDeviceToHost, s));
+    SHKZ_CUDA_TRY(cudaStreamSynchronize(s));
+    if (hst.done == 0) continue;
+    if (hst.done == 3 || hst.status == -5) { rc = SHKZ_B200_ERR_NAN; break; }
+    if (hst.done == 2) break;
+    if (hst.done == 1 && !reliable) break;
+    // reliable update: fold the FP32 increment into x64 and replace r by b - A x64
     launch_accumulate(n, ctx->x, scale, ctx->x64, s);
     launch_residual64(S, ctx->rhs64, ctx->x64, ctx->r64, ctx->partials, ctx->counter + 2, ctx->out4, s);
     SHKZ_CUDA_TRY(cudaMemcpyAsync(h4, ctx->out4, sizeof(h4), cudaMemcpyDeviceToHost, s));
     SHKZ_CUDA_TRY(cudaStreamSynchronize(s));
     rmax = h4[0];
     r2 = h4[1];
-    ++outer;
-    if (done == 3 || !(rmax == rmax)) { rc = SHKZ_B200_ERR_NAN; break; }
-    if (!ctx->cfg.refine) break;
+    ++updates;
+    true_checked = true;
+    if (!(rmax == rmax)) { rc = SHKZ_B200_ERR_NAN; break; }
     if (rmax <= tol * bmax) break;
-    if (iterations >= ctx->cfg.max_iterations) break;
-    if (done == 2) break;
+    launch_inner_init(n, ctx->r64, 1.0 / scale, ctx->r, ctx->x, s);
+    launch_state_resume(ctx->st, kReliableDrop * rmax / scale, s);
+    true_checked = false;
+    // complete the interrupted iteration with the replaced residual
+    launch_iteration_tail(ctx, S, n, precond, s);
+  }
+  if (!true_checked) {
+    // plain FP32 finish (refine off) or max iterations: report the true residual
+    launch_accumulate(n, ctx->x, scale, ctx->x64, s);
+    launch_residual64(S, ctx->rhs64, ctx->x64, ctx->r64, ctx->partials, ctx->counter + 2, ctx->out4, s);
+    SHKZ_CUDA_TRY(cudaMemcpyAsync(h4, ctx->out4, sizeof(h4), cudaMemcpyDeviceToHost, s));
+    SHKZ_CUDA_TRY(cudaStreamSynchronize(s));
+    rmax = h4[0];
+    r2 = h4[1];
   }
   if (wave_errors(ctx)) rc = SHKZ_B200_ERR_TIMEOUT;
-  res->iterations = iterations;
-  res->outer_steps = outer;
+  res->iterations = hst.iter;
+  res->outer_steps = updates;
   res->reresid = rmax / bmax;
   res->reresid_l2 = std::sqrt(r2 / b2);
   return rc;
@@ -433,8 +452,8 @@ static int fp64_reference_solve(shkz_b200_ctx *ctx, shkz_b200_result *res) {
   auto precond = [&](const double *r, double rmax) {
     // z = rmax * M^-1 (r / rmax) with M^-1 the FP32 MIC(0)
     launch_scale_f64_f32(n, r, 1.0 / rmax, ctx->r, s);
-    launch_mic_apply(S, ctx->d32, ctx->r, ctx->t, ctx->z, nullptr, ctx->wflags + ctx->cap_pool,
-                     ctx->wflags + 2 * ctx->cap_pool, wsync(ctx, 1), wsync(ctx, 2), nullptr, s);
+    launch_mic_apply(S, ctx->d32, ctx->r, ctx->t, ctx->z, nullptr, ctx->faces_f,
+                     ctx->faces_b, wsync(ctx, 1), wsync(ctx, 2), nullptr, s);
     launch_scale_f32_f64(n, ctx->z, rmax, ctx->z64, s);
   };
   SHKZ_CUDA_TRY(cudaMemsetAsync(ctx->xref64, 0, sizeof(double) * n, s));
@@ -764,8 +783,8 @@ static int dense_roundtrip(shkz_b200_ctx *ctx, const float *in_cells, float *out
     if (op == 0) {
       launch_spmv(S, ctx->r, ctx->z, ctx->partials, ctx->counter, nullptr, 1, s);
     } else if (ctx->cfg.preconditioner == SHKZ_B200_PRECOND_MIC0 || ctx->cfg.preconditioner == SHKZ_B200_PRECOND_LEARNED) {
-      launch_mic_apply(S, ctx->d32, ctx->r, ctx->t, ctx->z, nullptr, ctx->wflags + ctx->cap_pool,
-                       ctx->wflags + 2 * ctx->cap_pool, wsync(ctx, 1), wsync(ctx, 2), nullptr, s);
+      launch_mic_apply(S, ctx->d32, ctx->r, ctx->t, ctx->z, nullptr, ctx->faces_f,
+                       ctx->faces_b, wsync(ctx, 1), wsync(ctx, 2), nullptr, s);
     } else {
       cudaMemcpyAsync(ctx->z, ctx->r, sizeof(float) * n, cudaMemcpyDeviceToDevice, s);
     }
@@ -906,8 +925,8 @@ extern "C" int shkz_b200_time_kernel(shkz_b200_ctx *ctx, int which, int reps, do
       case 1:
       case 2: {
         // forward and backward are timed as a pair; the split uses two event pairs below
-        launch_mic_apply(S, ctx->d32, ctx->r, ctx->t, ctx->z, ctx->partials, ctx->wflags + ctx->cap_pool,
-                         ctx->wflags + 2 * ctx->cap_pool, wsync(ctx, 1), wsync(ctx, 2), nullptr, s);
+        launch_mic_apply(S, ctx->d32, ctx->r, ctx->t, ctx->z, ctx->partials, ctx->faces_f,
+                         ctx->faces_b, wsync(ctx, 1), wsync(ctx, 2), nullptr, s);
         break;
       }
       case 3: launch_update_xr(n, ctx->p, ctx->q, ctx->x, ctx->r, ctx->partials, ctx->counter + 1, ctx->st_scratch,
@@ -933,8 +952,8 @@ extern "C" int shkz_b200_time_kernel(shkz_b200_ctx *ctx, int which, int reps, do
     // time the two sweeps separately: forward then backward, each bracketed
     for (int i = 0; i < reps; ++i) {
       cudaEventRecord(ctx->ev[4], s);
-      launch_mic_apply(S, ctx->d32, ctx->r, ctx->t, ctx->z, ctx->partials, ctx->wflags + ctx->cap_pool,
-                       ctx->wflags + 2 * ctx->cap_pool, wsync(ctx, 1), wsync(ctx, 2), nullptr, s);
+      launch_mic_apply(S, ctx->d32, ctx->r, ctx->t, ctx->z, ctx->partials, ctx->faces_f,
+                       ctx->faces_b, wsync(ctx, 1), wsync(ctx, 2), nullptr, s);
       cudaEventRecord(ctx->ev[5], s);
       SHKZ_CUDA_TRY(cudaEventSynchronize(ctx->ev[5]));
       total += ms_between(ctx->ev[4], ctx->ev[5]);

@@ -38,8 +38,9 @@ struct SolverState {
   double rmax0;            // ||b||_inf
   double r2;               // ||r||_2^2
   double tol_abs;          // tol * ||b||_inf
+  double ru_threshold;     // request an FP64 residual replacement below this ||r||inf
   int iter;                // iterations completed
-  int done;                // 1 = converged, 2 = max iterations, 3 = breakdown
+  int done;                // 1 = converged, 2 = max iterations, 3 = breakdown, 4 = replace residual
   int status;              // 0 ok, <0 error (wait timeout, NaN)
   int pad;
 };

@@ -213,15 +213,28 @@ __device__ __forceinline__ void stage_tile(const PoolSystem &S, const float *__r
   }
 }
 
-// Computes the four outputs of this thread for tile pt (after staging and a barrier).
-__device__ __forceinline__ float4 stencil4(const PoolSystem &S, int pt, const SpmvSmem &sm, float4 xv) {
+struct Coef4 {
+  float4 dg, ox, oy, oz;
+};
+
+__device__ __forceinline__ Coef4 load_coef4(const PoolSystem &S, int pt) {
   const int tid = threadIdx.x;
   const int q4 = tid & 1, jj = (tid >> 1) & 7, kk = tid >> 4;
   const size_t base = (size_t)pt * SHKZ_TC + kk * 64 + jj * 8 + q4 * 4;
-  const float4 dg = ld4(S.diag + base);
-  const float4 ox = ld4(S.offx + base);
-  const float4 oy = ld4(S.offy + base);
-  const float4 oz = ld4(S.offz + base);
+  Coef4 c;
+  c.dg = ld4(S.diag + base);
+  c.ox = ld4(S.offx + base);
+  c.oy = ld4(S.offy + base);
+  c.oz = ld4(S.offz + base);
+  return c;
+}
+
+// Computes the four outputs of this thread for tile pt (after staging and a barrier).
+__device__ __forceinline__ float4 stencil4(const PoolSystem &S, int pt, const SpmvSmem &sm, float4 xv, const Coef4 &cf) {
+  const int tid = threadIdx.x;
+  const int q4 = tid & 1, jj = (tid >> 1) & 7, kk = tid >> 4;
+  const size_t base = (size_t)pt * SHKZ_TC + kk * 64 + jj * 8 + q4 * 4;
+  const float4 dg = cf.dg, ox = cf.ox, oy = cf.oy, oz = cf.oz;
   // upper weights: lower weights of the +x/+y/+z neighbour cells
   const float oxn = __shfl_down_sync(0xffffffffu, ox.x, 1);
   float4 oyn, ozn;
@@ -274,7 +287,7 @@ __device__ __forceinline__ float4 stencil4(const PoolSystem &S, int pt, const Sp
 
 // mode 0: q = A p and pq = p.q -> st->pq, st->alpha = rho/pq
 // mode 1: q = A p only
-__global__ void __launch_bounds__(128) k_spmv(PoolSystem S, const float *__restrict__ p, float *__restrict__ q,
+__global__ void __launch_bounds__(128, 10) k_spmv(PoolSystem S, const float *__restrict__ p, float *__restrict__ q,
                                               double *partials, unsigned *counter, SolverState *st, int mode) {
   __shared__ SpmvSmem sm;
   __shared__ double red[4];
@@ -284,10 +297,11 @@ __global__ void __launch_bounds__(128) k_spmv(PoolSystem S, const float *__restr
   const int q4 = tid & 1, jj = (tid >> 1) & 7, kk = tid >> 4;
   for (int pt = blockIdx.x; pt < S.K; pt += gridDim.x) {
     float4 xv;
+    const Coef4 cf = load_coef4(S, pt);
     __syncthreads();
     stage_tile(S, p, pt, sm, xv);
     __syncthreads();
-    const float4 y = stencil4(S, pt, sm, xv);
+    const float4 y = stencil4(S, pt, sm, xv, cf);
     st4(q + (size_t)pt * SHKZ_TC + kk * 64 + jj * 8 + q4 * 4, y);
     acc += (double)xv.x * y.x + (double)xv.y * y.y + (double)xv.z * y.z + (double)xv.w * y.w;
   }
@@ -349,6 +363,7 @@ __global__ void __launch_bounds__(256) k_update_xr(int n4, const float4 *__restr
       if (nan) { st->done = 3; st->status = -5; }
       else if (mm <= st->tol_abs) st->done = 1;
       else if (st->iter >= max_iterations) st->done = 2;
+      else if (mm < st->ru_threshold) st->done = 4;
       *counter = 0;
     }
   }
@@ -463,10 +478,12 @@ __device__ __forceinline__ void wave_begin(WaveSync *ws, int &slot, int &target)
   target = s_epoch;
 }
 
+// Producer side: every thread's stores precede the barrier; thread 0's
+// fence then orders them (cumulatively) before the releasing flag store.
 __device__ __forceinline__ void wave_end(WaveSync *ws, int *flags, int pt, int target) {
-  __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) {
+    __threadfence();
     st_release(&flags[pt], target);
     const unsigned f = atomicAdd(&ws->finished, 1u);
     if (f == gridDim.x - 1) {
@@ -487,8 +504,9 @@ __device__ __forceinline__ void wave_wait(WaveSync *ws, const int *flags, const 
       if (nb3[i] >= 0 && ok) ok = wait_flag(&flags[nb3[i]], target);
     if (!ok) atomicCAS(&ws->error, 0, slot + 1);
   }
+  // consumer side: thread 0's acquire, then the barrier, orders the other
+  // threads' (L2) loads of the neighbour tiles after the flag
   __syncthreads();
-  __threadfence();
 }
 
 // Tile rows are staged in shared memory; in step s of the in-tile wavefront
@@ -563,15 +581,60 @@ __global__ void __launch_bounds__(64) k_mic_factor(PoolSystem S, const int *sche
   wave_end(ws, flags, pt, target);
 }
 
-// Forward sweep t = d (r + sum_lower w t) in FP32.
+// Tile faces published with an epoch tag: entry = (epoch << 32) | float bits.
+// A 64-bit store is single-copy atomic, so a consumer that reads the current
+// epoch in an entry also reads that entry's value; no separate flag, fence or
+// second load is needed between neighbouring tiles.
+__device__ __forceinline__ void face_put(unsigned long long *e, int epoch, float v) {
+  const unsigned long long w = ((unsigned long long)(unsigned)epoch << 32) | (unsigned long long)__float_as_uint(v);
+  asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(e), "l"(w) : "memory");
+}
+// Bounded wait for the entry of the current epoch; returns its value (0 and
+// *ok = false when the limit was hit).
+__device__ __forceinline__ float face_get(const unsigned long long *e, int epoch, bool &ok) {
+  for (int it = 0; it < SPIN_LIMIT; ++it) {
+    unsigned long long w;
+    asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(w) : "l"(e) : "memory");
+    if ((int)(w >> 32) == epoch) return __uint_as_float((unsigned)(w & 0xffffffffu));
+    if (it > 32) __nanosleep(32);
+  }
+  ok = false;
+  return 0.0f;
+}
+
+__device__ __forceinline__ void sweep_begin(WaveSync *ws, int &slot, int &epoch) {
+  __shared__ int s_slot, s_epoch;
+  if (threadIdx.x == 0) {
+    s_slot = atomicAdd(&ws->slot, 1);
+    s_epoch = *((volatile int *)&ws->epoch) + 1;
+  }
+  __syncthreads();
+  slot = s_slot;
+  epoch = s_epoch;
+}
+
+__device__ __forceinline__ void sweep_end(WaveSync *ws, int epoch) {
+  if (threadIdx.x == 0) {
+    const unsigned f = atomicAdd(&ws->finished, 1u);
+    if (f == gridDim.x - 1) {
+      ws->slot = 0;
+      ws->finished = 0;
+      __threadfence();
+      atomicExch(&ws->epoch, epoch);
+    }
+  }
+}
+
+// Forward sweep t = d (r + sum_lower w t) in FP32. faces: [K][3][64]
+// (+x face ii=7 by jj+8kk, +y face jj=7 by ii+8kk, +z face kk=7 by ii+8jj).
 __global__ void __launch_bounds__(64) k_mic_forward(PoolSystem S, const int *sched, const float *__restrict__ d32,
-                                                    const float *__restrict__ r, float *__restrict__ t, int *flags,
-                                                    WaveSync *ws, const SolverState *st) {
+                                                    const float *__restrict__ r, float *__restrict__ t,
+                                                    unsigned long long *faces, WaveSync *ws, const SolverState *st) {
   __shared__ __align__(16) float T[SHKZ_TC], R[SHKZ_TC], Dd[SHKZ_TC], WX[SHKZ_TC], WY[SHKZ_TC], WZ[SHKZ_TC];
   __shared__ float hx[64], hy[64], hz[64];
   if (st && st->done) return;
-  int slot, target;
-  wave_begin(ws, slot, target);
+  int slot, epoch;
+  sweep_begin(ws, slot, epoch);
   const int pt = sched[slot];
   const int tid = threadIdx.x, jj = tid & 7, kk = tid >> 3;
   const size_t tb = (size_t)pt * SHKZ_TC;
@@ -580,13 +643,13 @@ __global__ void __launch_bounds__(64) k_mic_forward(PoolSystem S, const int *sch
   load_tile_f32(WX, S.offx + tb);
   load_tile_f32(WY, S.offy + tb);
   load_tile_f32(WZ, S.offz + tb);
-  const int nb3[3] = {S.nbr[pt * 6 + NB_XM], S.nbr[pt * 6 + NB_YM], S.nbr[pt * 6 + NB_ZM]};
-  wave_wait(ws, flags, nb3, target, slot);
   {
-    const int u = tid & 7, v = tid >> 3;
-    hx[tid] = nb3[0] >= 0 ? __ldcg(t + (size_t)nb3[0] * SHKZ_TC + 7 + 8 * u + 64 * v) : 0.0f;
-    hy[tid] = nb3[1] >= 0 ? __ldcg(t + (size_t)nb3[1] * SHKZ_TC + u + 56 + 64 * v) : 0.0f;
-    hz[tid] = nb3[2] >= 0 ? __ldcg(t + (size_t)nb3[2] * SHKZ_TC + u + 8 * v + 448) : 0.0f;
+    const int nxm = S.nbr[pt * 6 + NB_XM], nym = S.nbr[pt * 6 + NB_YM], nzm = S.nbr[pt * 6 + NB_ZM];
+    bool ok = true;
+    hx[tid] = nxm >= 0 ? face_get(faces + ((size_t)nxm * 3 + 0) * 64 + tid, epoch, ok) : 0.0f;
+    hy[tid] = nym >= 0 ? face_get(faces + ((size_t)nym * 3 + 1) * 64 + tid, epoch, ok) : 0.0f;
+    hz[tid] = nzm >= 0 ? face_get(faces + ((size_t)nzm * 3 + 2) * 64 + tid, epoch, ok) : 0.0f;
+    if (!ok) atomicCAS(&ws->error, 0, slot + 1);
   }
   __syncthreads();
   for (int s = 0; s < 22; ++s) {
@@ -600,23 +663,31 @@ __global__ void __launch_bounds__(64) k_mic_forward(PoolSystem S, const int *sch
     }
     __syncthreads();
   }
+  {
+    unsigned long long *f = faces + (size_t)pt * 3 * 64;
+    const int u = tid & 7, v = tid >> 3;
+    face_put(f + 0 * 64 + tid, epoch, T[7 + 8 * u + 64 * v]);
+    face_put(f + 1 * 64 + tid, epoch, T[u + 56 + 64 * v]);
+    face_put(f + 2 * 64 + tid, epoch, T[u + 8 * v + 448]);
+  }
   for (int v = tid; v < SHKZ_TC / 4; v += 64)
     reinterpret_cast<float4 *>(t + tb)[v] = reinterpret_cast<const float4 *>(T)[v];
-  wave_end(ws, flags, pt, target);
+  sweep_end(ws, epoch);
 }
 
 // Backward sweep z = t + d * sum_upper w z, reverse level order; fused z.r
-// partial per tile into partials[pt].
+// partial per tile into partials[pt]. faces: [K][3][64] (-x face ii=0,
+// -y face jj=0, -z face kk=0, same indexing as the forward faces).
 __global__ void __launch_bounds__(64) k_mic_backward(PoolSystem S, const int *sched, const float *__restrict__ d32,
                                                      const float *__restrict__ t, const float *__restrict__ r,
-                                                     float *__restrict__ z, double *partials, int *flags,
-                                                     WaveSync *ws, const SolverState *st) {
+                                                     float *__restrict__ z, double *partials,
+                                                     unsigned long long *faces, WaveSync *ws, const SolverState *st) {
   __shared__ __align__(16) float Z[SHKZ_TC], Tt[SHKZ_TC], Dd[SHKZ_TC], WX[SHKZ_TC], WY[SHKZ_TC], WZ[SHKZ_TC];
   __shared__ float hx[64], hy[64], hz[64], ux[64], uy[64], uz[64];
   __shared__ double red[2];
   if (st && st->done) return;
-  int slot, target;
-  wave_begin(ws, slot, target);
+  int slot, epoch;
+  sweep_begin(ws, slot, epoch);
   const int pt = sched[S.K - 1 - slot];
   const int tid = threadIdx.x, jj = tid & 7, kk = tid >> 3;
   const size_t tb = (size_t)pt * SHKZ_TC;
@@ -632,14 +703,11 @@ __global__ void __launch_bounds__(64) k_mic_backward(PoolSystem S, const int *sc
     ux[tid] = nxp >= 0 ? S.offx[(size_t)nxp * SHKZ_TC + 8 * u + 64 * v] : 0.0f;
     uy[tid] = nyp >= 0 ? S.offy[(size_t)nyp * SHKZ_TC + u + 64 * v] : 0.0f;
     uz[tid] = nzp >= 0 ? S.offz[(size_t)nzp * SHKZ_TC + u + 8 * v] : 0.0f;
-  }
-  const int nb3[3] = {nxp, nyp, nzp};
-  wave_wait(ws, flags, nb3, target, slot);
-  {
-    const int u = tid & 7, v = tid >> 3;
-    hx[tid] = nxp >= 0 ? __ldcg(z + (size_t)nxp * SHKZ_TC + 8 * u + 64 * v) : 0.0f;
-    hy[tid] = nyp >= 0 ? __ldcg(z + (size_t)nyp * SHKZ_TC + u + 64 * v) : 0.0f;
-    hz[tid] = nzp >= 0 ? __ldcg(z + (size_t)nzp * SHKZ_TC + u + 8 * v) : 0.0f;
+    bool ok = true;
+    hx[tid] = nxp >= 0 ? face_get(faces + ((size_t)nxp * 3 + 0) * 64 + tid, epoch, ok) : 0.0f;
+    hy[tid] = nyp >= 0 ? face_get(faces + ((size_t)nyp * 3 + 1) * 64 + tid, epoch, ok) : 0.0f;
+    hz[tid] = nzp >= 0 ? face_get(faces + ((size_t)nzp * 3 + 2) * 64 + tid, epoch, ok) : 0.0f;
+    if (!ok) atomicCAS(&ws->error, 0, slot + 1);
   }
   __syncthreads();
   for (int s = 21; s >= 0; --s) {
@@ -656,6 +724,13 @@ __global__ void __launch_bounds__(64) k_mic_backward(PoolSystem S, const int *sc
     }
     __syncthreads();
   }
+  {
+    unsigned long long *f = faces + (size_t)pt * 3 * 64;
+    const int u = tid & 7, v = tid >> 3;
+    face_put(f + 0 * 64 + tid, epoch, Z[8 * u + 64 * v]);
+    face_put(f + 1 * 64 + tid, epoch, Z[u + 64 * v]);
+    face_put(f + 2 * 64 + tid, epoch, Z[u + 8 * v]);
+  }
   double dot = 0.0;
   for (int v = tid; v < SHKZ_TC / 4; v += 64) {
     const float4 zv = reinterpret_cast<const float4 *>(Z)[v];
@@ -666,8 +741,9 @@ __global__ void __launch_bounds__(64) k_mic_backward(PoolSystem S, const int *sc
   #pragma unroll
   for (int o = 16; o > 0; o >>= 1) dot += __shfl_xor_sync(0xffffffffu, dot, o);
   if ((tid & 31) == 0) red[tid >> 5] = dot;
-  wave_end(ws, flags, pt, target);  // contains a barrier before the flag
+  __syncthreads();
   if (tid == 0 && partials) partials[pt] = red[0] + red[1];
+  sweep_end(ws, epoch);
 }
 
 // ---------------------------------------------------------------------------
@@ -803,9 +879,17 @@ __global__ void __launch_bounds__(256) k_inner_setup(int n, const float *__restr
       if (!(ss == ss)) st->done = 3;
       st->rho = 0.0;
       st->beta = 0.0;
+      st->ru_threshold = 0.0;
       *counter = 0;
     }
   }
+}
+
+// Host-directed state edits between batches (one thread).
+__global__ void k_state_resume(SolverState *st, double ru_threshold, int iter_offset) {
+  st->done = 0;
+  st->ru_threshold = ru_threshold;
+  (void)iter_offset;
 }
 
 // ---------------------------------------------------------------------------
@@ -976,12 +1060,13 @@ void launch_mic_factor(const PoolSystem &S, double *colsum, double omega, double
 }
 
 void launch_mic_apply(const PoolSystem &S, const float *d32, const float *r, float *t, float *z, double *partials,
-                      int *flags_f, int *flags_b, void *ws_f, void *ws_b, const SolverState *st, cudaStream_t s) {
+                      unsigned long long *faces_f, unsigned long long *faces_b, void *ws_f, void *ws_b,
+                      const SolverState *st, cudaStream_t s) {
   if (S.K <= 0) return;
   count_launches(1);
-  k_mic_forward<<<S.K, 64, 0, s>>>(S, S.sched, d32, r, t, flags_f, (WaveSync *)ws_f, st);
+  k_mic_forward<<<S.K, 64, 0, s>>>(S, S.sched, d32, r, t, faces_f, (WaveSync *)ws_f, st);
   count_launches(1);
-  k_mic_backward<<<S.K, 64, 0, s>>>(S, S.sched, d32, t, r, z, partials, flags_b, (WaveSync *)ws_b, st);
+  k_mic_backward<<<S.K, 64, 0, s>>>(S, S.sched, d32, t, r, z, partials, faces_b, (WaveSync *)ws_b, st);
 }
 
 void launch_residual64(const PoolSystem &S, const double *b, const double *x, double *r, double *partials,
@@ -1003,6 +1088,11 @@ void launch_to_float(int n, const double *a, float *b, cudaStream_t s) {
   count_launches(1);
   k_to_float<<<grid_for(n, 256 * 4, 148 * 8), 256, 0, s>>>(n, a, b);
 }
+void launch_state_resume(SolverState *st, double ru_threshold, cudaStream_t s) {
+  count_launches(1);
+  k_state_resume<<<1, 1, 0, s>>>(st, ru_threshold, 0);
+}
+
 void launch_inner_setup(int n, const float *r, double *partials, unsigned *counter, SolverState *st, double tol,
                         cudaStream_t s) {
   count_launches(1);

@@ -21,12 +21,14 @@ void launch_update_p(int n, const float *z, float *p, const SolverState *st, cud
 void launch_mic_factor(const PoolSystem &S, double *colsum, double omega, double min_ratio, double *d64, float *d32,
                        int *flags, void *ws, cudaStream_t s);
 void launch_mic_apply(const PoolSystem &S, const float *d32, const float *r, float *t, float *z, double *partials,
-                      int *flags_f, int *flags_b, void *ws_f, void *ws_b, const SolverState *st, cudaStream_t s);
+                      unsigned long long *faces_f, unsigned long long *faces_b, void *ws_f, void *ws_b,
+                      const SolverState *st, cudaStream_t s);
 void launch_residual64(const PoolSystem &S, const double *b, const double *x, double *r, double *partials,
                        unsigned *counter, double *out4, cudaStream_t s);
 void launch_inner_init(int n, const double *r64, double inv_scale, float *r32, float *x32, cudaStream_t s);
 void launch_accumulate(int n, const float *x32, double scale, double *x64, cudaStream_t s);
 void launch_to_float(int n, const double *a, float *b, cudaStream_t s);
+void launch_state_resume(SolverState *st, double ru_threshold, cudaStream_t s);
 void launch_inner_setup(int n, const float *r, double *partials, unsigned *counter, SolverState *st, double tol,
                         cudaStream_t s);
 

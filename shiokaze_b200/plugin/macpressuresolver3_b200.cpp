@@ -1,0 +1,234 @@
+/*
+ * macpressuresolver3_b200.cpp -- Shiokaze projection module backed by the
+ * B200 CUDA library.
+ *
+ * Drop-in for Projection=macpressuresolver3: select it with
+ * Projection=macpressuresolver3_b200 and the FLIP/APIC liquid and smoke
+ * timesteppers call it unchanged. It implements macproject3_interface
+ * (include/shiokaze/projection/macproject3_interface.h:42-113) with the
+ * meaning of macpressuresolver3 (src/projection/macpressuresolver3.cpp):
+ *   - reads the same configuration keys (Residual, MaxIterations,
+ *     ModifiedIC, MinDiagRatio, EpsFluid, EpsSolid,
+ *     SecondOrderAccurateFluid/Solid) plus B200.* keys;
+ *   - project() updates the face velocities in place, switches off the faces
+ *     the reference switches off, and keeps the pressure in an array3 that
+ *     get_pressure() returns;
+ *   - records the same timer labels and the iteration count under
+ *     <ArgName>_number_projection_iteration (macpressuresolver3.cpp:253).
+ * The host side only packs the array3/macarray3 grids into dense buffers and
+ * calls the C ABI (include/shkz_b200.h); all arithmetic runs on the GPU.
+ * Errors never throw: a failed solve is reported on the console and the
+ * record, and the velocity is left unprojected with 0 iterations recorded.
+ */
+#include <shiokaze/array/array3.h>
+#include <shiokaze/array/macarray3.h>
+#include <shiokaze/projection/macproject3_interface.h>
+#include <shiokaze/core/console.h>
+#include <shiokaze/core/timer.h>
+#include "shkz_b200.h"
+#include <cstring>
+#include <vector>
+//
+SHKZ_USING_NAMESPACE
+//
+class macpressuresolver3_b200 : public macproject3_interface {
+protected:
+	//
+	LONG_NAME("MAC Pressure Solver 3D (B200)")
+	//
+	virtual ~macpressuresolver3_b200() {
+		if( m_ctx ) shkz_b200_destroy(m_ctx);
+	}
+	//
+	virtual void set_target_volume( double current_volume, double target_volume ) override {
+		m_current_volume = current_volume;
+		m_target_volume = target_volume;
+	}
+	//
+	virtual void set_solid_density( const macarray3<Real> *solid_density ) override {
+		m_solid_density = solid_density;
+	}
+	//
+	template <class T> static void pack( const array3<T> &a, std::vector<float> &v, std::vector<uint8_t> &m ) {
+		const shape3 s = a.shape();
+		v.resize(s.count());
+		m.resize(s.count());
+		a.const_parallel_all([&]( int i, int j, int k, const typename array3<T>::const_iterator &it ) {
+			const size_t n = i+(size_t)s.w*(j+(size_t)s.h*k);
+			v[n] = (float)it();
+			m[n] = it.active() ? 1 : 0;
+		});
+	}
+	//
+	virtual void project( double dt,
+				macarray3<Real> &velocity,
+				const array3<Real> &solid,
+				const macarray3<Real> &solid_velocity,
+				const array3<Real> &fluid,
+				double surface_tension,
+				const std::vector<signed_rigidbody3_interface *> *rigidbodies ) override {
+		//
+		scoped_timer timer(this);
+		timer.tick(); console::dump( ">>> Pressure Projection (B200) started...\n" );
+		if( surface_tension || m_solid_density || (m_param.gain && m_target_volume) ) {
+			console::dump( "Surface tension, solid density and volume correction are not supported by the B200 projection; ignored.\n" );
+		}
+		if( ! m_ctx ) {
+			int rc = shkz_b200_create(&m_ctx,&m_cfg);
+			if( rc ) {
+				console::dump( "shkz_b200_create failed: %s\n", shkz_b200_errstr(rc));
+				console::write(get_argument_name()+"_number_projection_iteration", 0);
+				return;
+			}
+		} else {
+			shkz_b200_set_config(m_ctx,&m_cfg);
+		}
+		//
+		timer.tick(); console::dump( "Packing grids..." );
+		pack(fluid,m_fluid,m_fluid_active);
+		const bool has_solid = levelset_exist_any(solid);
+		if( has_solid ) pack(solid,m_solid,m_solid_active);
+		for( int dim=0; dim<3; ++dim ) {
+			pack(velocity[dim],m_vel[dim],m_vact[dim]);
+			pack(solid_velocity[dim],m_svel[dim],m_svact[dim]);
+		}
+		console::dump( "Done. Took %s\n", timer.stock("pack_grids").c_str());
+		//
+		shkz_b200_project_args a;
+		std::memset(&a,0,sizeof(a));
+		a.nx = m_shape.w; a.ny = m_shape.h; a.nz = m_shape.d;
+		a.dx = m_dx; a.dt = dt;
+		a.fluid = m_fluid.data(); a.fluid_active = m_fluid_active.data();
+		if( has_solid ) { a.solid = m_solid.data(); a.solid_active = m_solid_active.data(); }
+		for( int dim=0; dim<3; ++dim ) {
+			a.velocity[dim] = m_vel[dim].data();
+			a.velocity_active[dim] = m_vact[dim].data();
+			a.solid_velocity[dim] = m_svel[dim].data();
+		}
+		m_p.resize(m_shape.count());
+		m_pact.resize(m_shape.count());
+		a.pressure = m_p.data();
+		a.pressure_active = m_pact.data();
+		//
+		timer.tick(); console::dump( "Projecting on the GPU...");
+		shkz_b200_result res;
+		const int rc = shkz_b200_project_host(m_ctx,&a,&res);
+		console::write(get_argument_name()+"_number_projection_iteration", rc ? 0 : res.iterations);
+		console::write(get_argument_name()+"_reresid_inf", res.reresid);
+		console::write(get_argument_name()+"_reresid_l2", res.reresid_l2);
+		if( rc ) {
+			console::dump( "failed: %s (%s)\n", shkz_b200_errstr(rc), shkz_b200_last_error(m_ctx));
+			return;
+		}
+		console::dump( "Done. Took %d iterations, Reresid=%e. Took %s\n", res.iterations, res.reresid, timer.stock("linsolve").c_str());
+		//
+		timer.tick(); console::dump( "Updating the velocity...");
+		m_pressure.clear();
+		for( int k=0; k<m_shape.d; ++k ) for( int j=0; j<m_shape.h; ++j ) for( int i=0; i<m_shape.w; ++i ) {
+			const size_t n = i+(size_t)m_shape.w*(j+(size_t)m_shape.h*k);
+			if( m_pact[n] ) m_pressure.set(i,j,k,m_p[n]);
+		}
+		velocity.parallel_actives([&](int dim, int i, int j, int k, auto &it, int tn ) {
+			const shape3 fs = m_shape.face(dim);
+			const size_t n = i+(size_t)fs.w*(j+(size_t)fs.h*k);
+			if( m_vact[dim][n] ) it.set(m_vel[dim][n]);
+			else it.set_off();
+		});
+		console::dump( "Done. Took %s\n", timer.stock("update_velocity").c_str());
+		console::dump( "<<< Projection done. Took %s.\n", timer.stock("projection").c_str());
+	}
+	//
+	static bool levelset_exist_any( const array3<Real> &levelset ) {
+		bool inside (false);
+		levelset.interruptible_const_serial_actives([&](int i, int j, int k, const auto &it) {
+			if( it() < 0.0 ) inside = true;
+			return inside;
+		});
+		return inside;
+	}
+	//
+	virtual void configure( configuration &config ) override {
+		config.get_bool("SecondOrderAccurateFluid",m_param.second_order_accurate_fluid,"Whether to enforce second order accuracy");
+		config.get_bool("SecondOrderAccurateSolid",m_param.second_order_accurate_solid,"Whether to enforce second order accuracy for solid surfaces");
+		config.get_double("Gain",m_param.gain,"Rate for volume correction");
+		config.get_double("Residual",m_cfg.residual,"Tolerable residual");
+		unsigned max_it = m_cfg.max_iterations;
+		config.get_unsigned("MaxIterations",max_it,"Maximal iteration count");
+		m_cfg.max_iterations = max_it;
+		config.get_double("ModifiedIC",m_cfg.mic_omega,"Modified incomplete cholesky");
+		config.get_double("MinDiagRatio",m_cfg.mic_min_diag_ratio,"Minimal diagonal ratio");
+		config.get_double("EpsFluid",m_cfg.eps_fluid,"Minimal bound for fluid fraction");
+		config.get_double("EpsSolid",m_cfg.eps_solid,"Minimal bound for solid fraction");
+		std::string pre ("mic0");
+		config.get_string("B200.Preconditioner",pre,"none, mic0 or learned");
+		m_cfg.preconditioner = pre == "none" ? SHKZ_B200_PRECOND_NONE : (pre == "learned" ? SHKZ_B200_PRECOND_LEARNED : SHKZ_B200_PRECOND_MIC0);
+		bool refine = m_cfg.refine;
+		config.get_bool("B200.Refine",refine,"FP64 refinement of the FP32 solve");
+		m_cfg.refine = refine;
+		int device = m_cfg.device;
+		config.get_integer("B200.Device",device,"CUDA device ordinal");
+		m_cfg.device = device;
+		m_cfg.second_order_fluid = m_param.second_order_accurate_fluid;
+		m_cfg.second_order_solid = m_param.second_order_accurate_solid;
+	}
+	virtual void initialize( const shape3 &shape, double dx ) override {
+		m_shape = shape;
+		m_dx = dx;
+	}
+	virtual void post_initialize( bool initialized_from_file ) override {
+		m_pressure.initialize(m_shape);
+		m_target_volume = m_current_volume = m_y_prev = 0.0;
+	}
+	// Same fields in the same order as macpressuresolver3 (:320-342), so
+	// saved states load in either module (warm start is not supported here).
+	virtual void initialize( const filestream &file ) override {
+		file.r(m_shape);
+		file.r(m_dx);
+		file.r(m_target_volume);
+		file.r(m_current_volume);
+		file.r(m_y_prev);
+	}
+	virtual void serialize( const filestream &file ) const override {
+		file.w(m_shape);
+		file.w(m_dx);
+		file.w(m_target_volume);
+		file.w(m_current_volume);
+		file.w(m_y_prev);
+	}
+	virtual const array3<Real> * get_pressure() const override {
+		return &m_pressure;
+	}
+	//
+	struct Parameters {
+		double gain {1.0};
+		bool second_order_accurate_fluid {true};
+		bool second_order_accurate_solid {true};
+	};
+	Parameters m_param;
+	shkz_b200_config m_cfg = make_default_config();
+	static shkz_b200_config make_default_config() {
+		shkz_b200_config c;
+		shkz_b200_default_config(&c);
+		return c;
+	}
+	shkz_b200_ctx *m_ctx {nullptr};
+	//
+	shape3 m_shape;
+	double m_dx {0.0};
+	array3<Real> m_pressure{this};
+	double m_target_volume {0.0};
+	double m_current_volume {0.0};
+	double m_y_prev {0.0};
+	const macarray3<Real> *m_solid_density {nullptr};
+	// host staging
+	std::vector<float> m_fluid, m_solid, m_vel[3], m_svel[3], m_p;
+	std::vector<uint8_t> m_fluid_active, m_solid_active, m_vact[3], m_svact[3], m_pact;
+};
+//
+extern "C" module * create_instance() {
+	return new macpressuresolver3_b200();
+}
+//
+extern "C" const char *license() {
+	return "MIT";
+}
