@@ -177,6 +177,40 @@ int shkz_b200_apply_matrix(shkz_b200_ctx *ctx, const float *x_cells, float *y_ce
  * roofline figures. */
 int shkz_b200_time_kernel(shkz_b200_ctx *ctx, int which, int reps, double *ms_per_launch, long long *cells_out);
 
+/* ---- learned preconditioner (conv encoder-decoder, see DESIGN) ----
+ * No counterpart in the reference: the network is the second preconditioner
+ * of the projection (config preconditioner = SHKZ_B200_PRECOND_LEARNED);
+ * the entry points below create, train, inspect and persist it. Training and
+ * inspection act on the system of the last projection. */
+int shkz_b200_learned_init(shkz_b200_ctx *ctx, unsigned seed);
+long long shkz_b200_learned_param_count(shkz_b200_ctx *ctx);
+/* parameters blob: per layer w[27][cout][cin] then b[cout], FP32 */
+int shkz_b200_learned_set_params(shkz_b200_ctx *ctx, const float *blob, size_t n);
+int shkz_b200_learned_get_params(shkz_b200_ctx *ctx, float *blob, size_t n, int gradients);
+/* z = s N(r / s), s = ||r||inf, for a dense host residual (f32 cells) */
+int shkz_b200_learned_apply(shkz_b200_ctx *ctx, const float *r_cells, float *z_cells);
+/* dense level-0 network grid (cells rounded up to multiples of 4) */
+int shkz_b200_learned_dims(shkz_b200_ctx *ctx, int *dims);
+/* which = 0..12: stored activations X0, A1, S1, P1, A2, S2, P2, A3, B3, C2,
+ * D2, C1, D1 (dense channels-last f32); 13: raw output Z; 14..26: gradients
+ * w.r.t. activations 0..12 after the last backward. shape4 (may be
+ * NULL) receives z, y, x, channels; out may be NULL to query the shape. */
+int shkz_b200_learned_tensor(shkz_b200_ctx *ctx, int which, float *out, size_t count, int *shape4);
+/* weight gradients of sum(gZ * Z) for the last application */
+int shkz_b200_learned_backward(shkz_b200_ctx *ctx, const float *gZ_dense, size_t count);
+/* `steps` Adam steps (learning rate lr) on the energy loss 1/2 z.Az - z.r */
+int shkz_b200_learned_train(shkz_b200_ctx *ctx, int steps, double lr, unsigned seed, double *losses);
+int shkz_b200_learned_save(shkz_b200_ctx *ctx, const char *path);
+/* One 3^3 convolution of the network's tensor-core kernel on host arrays
+ * (checking the kernel in isolation): in0 (nz,ny,nx,c0), in1 at half
+ * resolution (nz/2,ny/2,nx/2,c1) nearest-upsampled and concatenated (may be
+ * NULL when c1 = 0), w[27][cout][c0+c1], bias[cout] (may be NULL), planes = 4
+ * or 8 output z planes per CTA; out (nz,ny,nx,cout). c0, c1 multiples of 16,
+ * cout <= 128, even grid sizes. No reference counterpart. */
+int shkz_b200_conv3d(int nx, int ny, int nz, int c0, int c1, int cout, int planes, const float *in0,
+                     const float *in1, const float *w, const float *bias, int relu, float *out);
+int shkz_b200_learned_load(shkz_b200_ctx *ctx, const char *path);
+
 #ifdef __cplusplus
 }
 #endif

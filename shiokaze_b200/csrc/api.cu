@@ -67,6 +67,7 @@ struct shkz_b200_ctx {
   long long unknowns = 0;
   int has_system = 0;
   LearnedModel *model = nullptr;
+  int model_ready = 0;  // block activity computed for the current system
   AssemblyInputs last_in{};
   SolverState *st_scratch = nullptr;
 };
@@ -503,6 +504,8 @@ static int fp64_reference_solve(shkz_b200_ctx *ctx, shkz_b200_result *res) {
   return 0;
 }
 
+static int learned_solve(shkz_b200_ctx *ctx, double tol, shkz_b200_result *res);
+
 static int validate(const shkz_b200_project_args *a) {
   if (!a || a->nx <= 0 || a->ny <= 0 || a->nz <= 0 || !a->fluid || !a->fluid_active) return SHKZ_B200_ERR_ARG;
   if (a->nx > 65536 || a->ny > 65536 || a->nz > 65536) return SHKZ_B200_ERR_LIMIT;
@@ -559,6 +562,7 @@ static int project_device(shkz_b200_ctx *ctx, const shkz_b200_project_args *a, s
   SHKZ_CUDA_TRY(cudaGetLastError());
   ctx->K = K;
   ctx->G = G;
+  ctx->model_ready = 0;
   res->tiles = K;
   CoeffOutputs co{ctx->diag, ctx->offx, ctx->offy, ctx->offz, ctx->diag64, ctx->offx64, ctx->offy64, ctx->offz64,
                   ctx->rhs64};
@@ -584,7 +588,7 @@ static int project_device(shkz_b200_ctx *ctx, const shkz_b200_project_args *a, s
   int solve_rc = 0;
   if (K > 0) {
     if (precond == SHKZ_B200_PRECOND_LEARNED && ctx->model)
-      solve_rc = learned_solve(ctx->model, ctx, res);
+      solve_rc = learned_solve(ctx, ctx->cfg.residual, res);
     else
       solve_rc = solve_system(ctx, ctx->cfg.residual, precond == SHKZ_B200_PRECOND_LEARNED ? SHKZ_B200_PRECOND_MIC0 : precond, res);
   } else {
@@ -970,4 +974,357 @@ extern "C" int shkz_b200_time_kernel(shkz_b200_ctx *ctx, int which, int reps, do
   if (cells_out) *cells_out = (which == 5) ? (long long)ctx->G.nx * ctx->G.ny * ctx->G.nz : (long long)n;
   if (wave_errors(ctx)) return SHKZ_B200_ERR_TIMEOUT;
   return 0;
+}
+
+// --------------------------------------------------------------------------
+// Learned preconditioner: flexible PCG and the model entry points
+
+static LearnedSystem learned_system(shkz_b200_ctx *ctx) {
+  LearnedSystem L;
+  L.G = ctx->G;
+  L.tile_state = ctx->tile_state;
+  L.pool_tile = ctx->pool_tile;
+  L.K = ctx->K;
+  L.unk = ctx->unk;
+  L.fluid = ctx->last_in.fluid;
+  L.solid = ctx->last_in.solid;
+  L.dx = ctx->last_in.dx;
+  return L;
+}
+
+static int learned_ready(shkz_b200_ctx *ctx) {
+  if (!ctx->model) return SHKZ_B200_ERR_STATE;
+  if (!ctx->has_system) return SHKZ_B200_ERR_STATE;
+  if (!ctx->model_ready) {
+    int rc = learned_prepare(ctx->model, ctx->G, ctx->tile_state, ctx->stream);
+    if (rc) return rc;
+    ctx->model_ready = 1;
+  }
+  return 0;
+}
+
+// Flexible PCG (Polak-Ribiere beta) with the learned preconditioner on FP32
+// vectors, FP64 reductions and reliable updates (as solve_system). When the
+// residual stalls -- less than a 10 % reduction over `stall_window`
+// iterations -- the solve falls back to the reference's MIC(0) for the rest
+// of the solve and restarts the direction from the current residual.
+static int learned_solve(shkz_b200_ctx *ctx, double tol, shkz_b200_result *res) {
+  int rc = learned_ready(ctx);
+  if (rc) return rc;
+  cudaStream_t s = ctx->stream;
+  const PoolSystem S = pool_system(ctx);
+  const LearnedSystem LS = learned_system(ctx);
+  const int n = ctx->K * SHKZ_TC;
+  SHKZ_CUDA_TRY(cudaMemsetAsync(ctx->x64, 0, sizeof(double) * n, s));
+  double h4[4];
+  launch_residual64(S, ctx->rhs64, ctx->x64, ctx->r64, ctx->partials, ctx->counter + 2, ctx->out4, s);
+  SHKZ_CUDA_TRY(cudaMemcpyAsync(h4, ctx->out4, sizeof(h4), cudaMemcpyDeviceToHost, s));
+  SHKZ_CUDA_TRY(cudaStreamSynchronize(s));
+  const double bmax = h4[2], b2 = h4[3];
+  double rmax_true = h4[0], r2 = h4[1];
+  res->outer_steps = 0;
+  res->fallbacks = 0;
+  if (bmax == 0.0) {
+    res->iterations = 0;
+    res->reresid = 0.0;
+    res->reresid_l2 = 0.0;
+    return 0;
+  }
+  const double scale = bmax;
+  launch_inner_init(n, ctx->r64, 1.0 / scale, ctx->r, ctx->x, s);
+  launch_inner_setup(n, ctx->r, ctx->partials, ctx->counter, ctx->st, tol, s);
+  launch_state_resume(ctx->st, kReliableDrop, s);
+  bool use_mic = false;
+  auto precondition = [&](double rmax_scaled) -> int {
+    if (use_mic) {
+      launch_mic_apply(S, ctx->d32, ctx->r, ctx->t, ctx->z, nullptr, ctx->faces_f, ctx->faces_b, wsync(ctx, 1),
+                       wsync(ctx, 2), ctx->st, s);
+      return 0;
+    }
+    return learned_apply(ctx->model, LS, ctx->r, rmax_scaled, ctx->z, s);
+  };
+  if ((rc = precondition(1.0))) return rc;
+  launch_fpcg_dots(n, ctx->z, ctx->r, ctx->q, ctx->partials, ctx->counter + 5, ctx->st, 1, s);
+  SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->p, ctx->z, sizeof(float) * n, cudaMemcpyDeviceToDevice, s));
+  const int max_it = ctx->cfg.max_iterations;
+  const int W = ctx->cfg.stall_window > 0 ? ctx->cfg.stall_window : 8;
+  std::vector<double> hist;
+  SolverState hst;
+  int updates = 0;
+  bool true_checked = false;
+  for (;;) {
+    launch_spmv(S, ctx->p, ctx->q, ctx->partials, ctx->counter, ctx->st, 0, s);
+    launch_update_xr(n, ctx->p, ctx->q, ctx->x, ctx->r, ctx->partials, ctx->counter + 1, ctx->st, max_it, s);
+    SHKZ_CUDA_TRY(cudaMemcpyAsync(&hst, ctx->st, sizeof(hst), cudaMemcpyDeviceToHost, s));
+    SHKZ_CUDA_TRY(cudaStreamSynchronize(s));
+    if (hst.done == 3 || hst.status == -5) { rc = SHKZ_B200_ERR_NAN; break; }
+    if (hst.done == 2) break;
+    true_checked = false;
+    double rmax = hst.rmax;
+    if (hst.done == 1 || hst.done == 4) {
+      launch_accumulate(n, ctx->x, scale, ctx->x64, s);
+      launch_residual64(S, ctx->rhs64, ctx->x64, ctx->r64, ctx->partials, ctx->counter + 2, ctx->out4, s);
+      SHKZ_CUDA_TRY(cudaMemcpyAsync(h4, ctx->out4, sizeof(h4), cudaMemcpyDeviceToHost, s));
+      SHKZ_CUDA_TRY(cudaStreamSynchronize(s));
+      rmax_true = h4[0];
+      r2 = h4[1];
+      ++updates;
+      true_checked = true;
+      if (!(rmax_true == rmax_true)) { rc = SHKZ_B200_ERR_NAN; break; }
+      if (rmax_true <= tol * bmax) break;
+      launch_inner_init(n, ctx->r64, 1.0 / scale, ctx->r, ctx->x, s);
+      launch_state_resume(ctx->st, kReliableDrop * rmax_true / scale, s);
+      rmax = rmax_true / scale;
+    }
+    hist.push_back(rmax);
+    const int k = (int)hist.size() - 1;
+    bool restart = false;
+    if (!use_mic && k >= W && rmax > 0.9 * hist[k - W]) {
+      use_mic = true;  // stall: fall back to MIC(0)
+      res->fallbacks += 1;
+      restart = true;
+    }
+    if ((rc = precondition(rmax))) break;
+    launch_fpcg_dots(n, ctx->z, ctx->r, ctx->q, ctx->partials, ctx->counter + 5, ctx->st, restart ? 1 : 0, s);
+    if (restart) SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->p, ctx->z, sizeof(float) * n, cudaMemcpyDeviceToDevice, s));
+    else launch_update_p(n, ctx->z, ctx->p, ctx->st, s);
+  }
+  if (!true_checked && rc == 0) {
+    launch_accumulate(n, ctx->x, scale, ctx->x64, s);
+    launch_residual64(S, ctx->rhs64, ctx->x64, ctx->r64, ctx->partials, ctx->counter + 2, ctx->out4, s);
+    SHKZ_CUDA_TRY(cudaMemcpyAsync(h4, ctx->out4, sizeof(h4), cudaMemcpyDeviceToHost, s));
+    SHKZ_CUDA_TRY(cudaStreamSynchronize(s));
+    rmax_true = h4[0];
+    r2 = h4[1];
+  }
+  if (!rc && learned_error(ctx->model)) rc = SHKZ_B200_ERR_TIMEOUT;
+  if (!rc && wave_errors(ctx)) rc = SHKZ_B200_ERR_TIMEOUT;
+  res->iterations = hst.iter;
+  res->outer_steps = updates;
+  res->reresid = rmax_true / bmax;
+  res->reresid_l2 = std::sqrt(r2 / b2);
+  return rc;
+}
+
+extern "C" int shkz_b200_learned_init(shkz_b200_ctx *ctx, unsigned seed) {
+  if (!ctx) return SHKZ_B200_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  if (!ctx->model) {
+    ctx->model = learned_create(ctx->device);
+    if (!ctx->model) return SHKZ_B200_ERR_NOMEM;
+  }
+  ctx->model_ready = 0;
+  return learned_init_params(ctx->model, seed, ctx->stream);
+}
+
+extern "C" long long shkz_b200_learned_param_count(shkz_b200_ctx *ctx) {
+  return (ctx && ctx->model) ? (long long)learned_param_count(ctx->model) : -1;
+}
+
+extern "C" int shkz_b200_learned_set_params(shkz_b200_ctx *ctx, const float *blob, size_t n) {
+  if (!ctx || !blob) return SHKZ_B200_ERR_ARG;
+  if (!ctx->model) return SHKZ_B200_ERR_STATE;
+  cudaSetDevice(ctx->device);
+  return learned_set_params(ctx->model, blob, n, ctx->stream);
+}
+
+extern "C" int shkz_b200_learned_get_params(shkz_b200_ctx *ctx, float *blob, size_t n, int gradients) {
+  if (!ctx || !blob) return SHKZ_B200_ERR_ARG;
+  if (!ctx->model) return SHKZ_B200_ERR_STATE;
+  cudaSetDevice(ctx->device);
+  return learned_get_params(ctx->model, blob, n, gradients, ctx->stream);
+}
+
+// z = s N(r/s) at unknown cells for a dense host residual (FP32 cells).
+extern "C" int shkz_b200_learned_apply(shkz_b200_ctx *ctx, const float *r_cells, float *z_cells) {
+  if (!ctx || !r_cells || !z_cells) return SHKZ_B200_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  int rc = learned_ready(ctx);
+  if (rc) return rc;
+  cudaStream_t s = ctx->stream;
+  const Geometry &G = ctx->G;
+  const size_t cells = (size_t)G.nx * G.ny * G.nz;
+  double rmax = 0.0;
+  for (size_t i = 0; i < cells; ++i) rmax = std::fmax(rmax, std::fabs((double)r_cells[i]));
+  float *dense = nullptr;
+  SHKZ_CUDA_TRY(cudaMalloc(&dense, cells * 4));
+  cudaMemcpyAsync(dense, r_cells, cells * 4, cudaMemcpyHostToDevice, s);
+  if (ctx->K > 0) {
+    count_launches(1);
+    k_dense_to_pool_f32<<<148 * 8, 256, 0, s>>>(G, ctx->pool_tile, ctx->K, dense, ctx->r);
+    rc = learned_apply(ctx->model, learned_system(ctx), ctx->r, rmax, ctx->z, s);
+    count_launches(1);
+    k_pool_to_dense_f32<<<148 * 8, 256, 0, s>>>(G, ctx->tile_state, ctx->z, dense);
+  }
+  cudaError_t e = cudaMemcpyAsync(z_cells, dense, cells * 4, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFree(dense);
+  if (e != cudaSuccess) {
+    shkz_set_cuda_error(e, "learned_apply", __FILE__, __LINE__);
+    return SHKZ_B200_ERR_CUDA;
+  }
+  if (!rc) rc = learned_error(ctx->model);
+  return rc;
+}
+
+// Dense level-0 network dimensions (grid rounded up to multiples of 4).
+extern "C" int shkz_b200_learned_dims(shkz_b200_ctx *ctx, int *dims) {
+  if (!ctx || !dims) return SHKZ_B200_ERR_ARG;
+  int rc = learned_ready(ctx);
+  if (rc) return rc;
+  learned_dense_dims(ctx->model, &dims[0], &dims[1], &dims[2]);
+  return 0;
+}
+
+// Inspection of the last network application: which = 0 .. 12 are the
+// stored activations X0, A1, S1, P1, A2, S2, P2, A3, B3, C2, D2, C1, D1
+// (dense channels-last FP32, shape4 = z, y, x, channels); which = 13 is the
+// raw FP32 output Z of the last layer (channels = 1); 14 .. 26 are the
+// FP32 gradients w.r.t. tensors 0 .. 12 after the last backward pass.
+extern "C" int shkz_b200_learned_tensor(shkz_b200_ctx *ctx, int which, float *out, size_t count, int *shape4) {
+  if (!ctx || which < 0 || which > 26) return SHKZ_B200_ERR_ARG;
+  int rc = learned_ready(ctx);
+  if (rc) return rc;
+  cudaStream_t s = ctx->stream;
+  size_t need;
+  int shp[4];
+  if (which == 13) {
+    learned_tensor_shape(ctx->model, 0, shp);
+    shp[3] = 1;
+    need = learned_dense_cells(ctx->model);
+  } else {
+    learned_tensor_shape(ctx->model, which % 14, shp);
+    need = learned_tensor_size(ctx->model, which % 14);
+  }
+  if (shape4) std::memcpy(shape4, shp, sizeof(shp));
+  if (!out) return 0;
+  if (count < need) return SHKZ_B200_ERR_ARG;
+  float *d = nullptr;
+  SHKZ_CUDA_TRY(cudaMalloc(&d, need * 4));
+  rc = which == 13 ? learned_output_dense(ctx->model, d, s)
+                   : (which > 13 ? learned_grad_dense(ctx->model, which - 14, d, s)
+                                 : learned_tensor_dense(ctx->model, which, d, s));
+  cudaError_t e = cudaMemcpyAsync(out, d, need * 4, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFree(d);
+  if (e != cudaSuccess) return SHKZ_B200_ERR_CUDA;
+  return rc;
+}
+
+// Weight gradients of sum(gZ * Z) for the last application (gZ dense level-0 FP32, host).
+extern "C" int shkz_b200_learned_backward(shkz_b200_ctx *ctx, const float *gZ_dense, size_t count) {
+  if (!ctx || !gZ_dense) return SHKZ_B200_ERR_ARG;
+  int rc = learned_ready(ctx);
+  if (rc) return rc;
+  cudaStream_t s = ctx->stream;
+  const size_t nv = learned_dense_cells(ctx->model);
+  if (count < nv) return SHKZ_B200_ERR_ARG;
+  float *d = nullptr;
+  SHKZ_CUDA_TRY(cudaMalloc(&d, nv * 4));
+  cudaMemcpyAsync(d, gZ_dense, nv * 4, cudaMemcpyHostToDevice, s);
+  rc = learned_backward_dense(ctx->model, d, s);
+  cudaError_t e = cudaStreamSynchronize(s);
+  cudaFree(d);
+  if (e != cudaSuccess) return SHKZ_B200_ERR_CUDA;
+  if (!rc) rc = learned_error(ctx->model);
+  return rc;
+}
+
+// Training on the last projection's system: step i uses a residual that is
+// the right-hand side (i % 3 == 0), A e for white noise e (i % 3 == 1), or
+// b + A e (i % 3 == 2), scaled to ||r||inf = 1; energy loss, Adam(lr).
+extern "C" int shkz_b200_learned_train(shkz_b200_ctx *ctx, int steps, double lr, unsigned seed, double *losses) {
+  if (!ctx || steps < 0) return SHKZ_B200_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  int rc = learned_ready(ctx);
+  if (rc) return rc;
+  if (ctx->K == 0) return 0;
+  cudaStream_t s = ctx->stream;
+  const PoolSystem S = pool_system(ctx);
+  const LearnedSystem LS = learned_system(ctx);
+  const int n = ctx->K * SHKZ_TC;
+  for (int i = 0; i < steps; ++i) {
+    const int kind = i % 3;
+    // r (FP32 pool) in ctx->r; scratch: ctx->t (noise), ctx->q (A e)
+    if (kind != 1) launch_to_float(n, ctx->rhs64, ctx->r, s);
+    else SHKZ_CUDA_TRY(cudaMemsetAsync(ctx->r, 0, sizeof(float) * n, s));
+    if (kind != 0) {
+      launch_rand_unknowns(n, ctx->diag, seed * 7919u + (unsigned)i, ctx->t, s);
+      launch_spmv(S, ctx->t, ctx->q, ctx->partials, ctx->counter, nullptr, 1, s);
+      // balance the two parts by their sizes
+      launch_inner_setup(n, ctx->q, ctx->partials, ctx->counter, ctx->st_scratch, 1.0, s);
+      SolverState a1;
+      cudaMemcpyAsync(&a1, ctx->st_scratch, sizeof(a1), cudaMemcpyDeviceToHost, s);
+      launch_inner_setup(n, ctx->r, ctx->partials, ctx->counter, ctx->st_scratch, 1.0, s);
+      SolverState a2;
+      cudaMemcpyAsync(&a2, ctx->st_scratch, sizeof(a2), cudaMemcpyDeviceToHost, s);
+      SHKZ_CUDA_TRY(cudaStreamSynchronize(s));
+      const float w = (kind == 1 || a1.rmax0 == 0.0) ? 1.0f : (float)(a2.rmax0 / a1.rmax0);
+      launch_axpby_f32(n, w, ctx->q, 1.0f, ctx->r, s);
+    }
+    launch_inner_setup(n, ctx->r, ctx->partials, ctx->counter, ctx->st_scratch, 1.0, s);
+    SolverState a3;
+    SHKZ_CUDA_TRY(cudaMemcpyAsync(&a3, ctx->st_scratch, sizeof(a3), cudaMemcpyDeviceToHost, s));
+    SHKZ_CUDA_TRY(cudaStreamSynchronize(s));
+    if (a3.rmax0 > 0) launch_scale_f32(n, ctx->r, (float)(1.0 / a3.rmax0), s);
+    double loss = 0.0;
+    rc = learned_train_step(ctx->model, LS, S, ctx->r, ctx->z, ctx->q, ctx->partials, ctx->counter, (float)lr, &loss, s);
+    if (rc) return rc;
+    if (losses) losses[i] = loss;
+  }
+  return 0;
+}
+
+extern "C" int shkz_b200_learned_save(shkz_b200_ctx *ctx, const char *path) {
+  if (!ctx || !path) return SHKZ_B200_ERR_ARG;
+  if (!ctx->model) return SHKZ_B200_ERR_STATE;
+  const size_t n = learned_param_count(ctx->model);
+  std::vector<float> blob(n);
+  int rc = learned_get_params(ctx->model, blob.data(), n, 0, ctx->stream);
+  if (rc) return rc;
+  FILE *f = std::fopen(path, "wb");
+  if (!f) return SHKZ_B200_ERR_ARG;
+  const unsigned long long nn = n;
+  std::fwrite("SHKZNET1", 1, 8, f);
+  std::fwrite(&nn, 8, 1, f);
+  std::fwrite(blob.data(), 4, n, f);
+  std::fclose(f);
+  return 0;
+}
+
+extern "C" int shkz_b200_learned_load(shkz_b200_ctx *ctx, const char *path) {
+  if (!ctx || !path) return SHKZ_B200_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  if (!ctx->model) {
+    ctx->model = learned_create(ctx->device);
+    if (!ctx->model) return SHKZ_B200_ERR_NOMEM;
+  }
+  FILE *f = std::fopen(path, "rb");
+  if (!f) return SHKZ_B200_ERR_ARG;
+  char magic[8];
+  unsigned long long nn = 0;
+  const bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "SHKZNET1", 8) == 0 &&
+                  std::fread(&nn, 8, 1, f) == 1 && nn == learned_param_count(ctx->model);
+  if (!ok) {
+    std::fclose(f);
+    return SHKZ_B200_ERR_ARG;
+  }
+  std::vector<float> blob(nn);
+  const size_t got = std::fread(blob.data(), 4, nn, f);
+  std::fclose(f);
+  if (got != nn) return SHKZ_B200_ERR_ARG;
+  ctx->model_ready = 0;
+  return learned_set_params(ctx->model, blob.data(), nn, ctx->stream);
+}
+
+// One 3^3 convolution on the tensor cores with host arrays (unit tests of the
+// kernel): in0 (nz,ny,nx,c0), in1 (nz/2,ny/2,nx/2,c1) nearest-upsampled and
+// concatenated, w[27][cout][c0+c1], bias[cout] (may be NULL); out (nz,ny,nx,cout),
+// BF16-rounded values as FP32.
+extern "C" int shkz_b200_conv3d(int nx, int ny, int nz, int c0, int c1, int cout, int planes, const float *in0,
+                                const float *in1, const float *w, const float *bias, int relu, float *out) {
+  if (nx <= 0 || ny <= 0 || nz <= 0 || c0 <= 0 || c0 % 16 || c1 < 0 || c1 % 16 || cout <= 0 || cout > 128 ||
+      (planes != 4 && planes != 8) || !in0 || !w || !out || (c1 && !in1) || (nx | ny | nz) & 1)
+    return SHKZ_B200_ERR_ARG;
+  return conv3d_run(nx, ny, nz, c0, c1, cout, planes, in0, in1, w, bias, relu, out);
 }

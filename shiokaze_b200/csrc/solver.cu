@@ -976,6 +976,79 @@ __global__ void __launch_bounds__(256) k_scale_f32_f64(int n, const float *__res
 }
 
 // ---------------------------------------------------------------------------
+// Flexible PCG pieces (learned preconditioner)
+
+// z.r and z.q (FP64); init: rho = z.r, beta = 0; else Polak-Ribiere
+// beta = z.(r_new - r_old)/rho = -alpha z.q / rho (r_old = r_new + alpha q).
+__global__ void __launch_bounds__(256) k_fpcg_dots(int n4, const float4 *__restrict__ z, const float4 *__restrict__ r,
+                                                   const float4 *__restrict__ q, double *partials, unsigned *counter,
+                                                   SolverState *st, int init) {
+  __shared__ double red[8];
+  if (st->done) return;
+  double a = 0.0, b = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += gridDim.x * blockDim.x) {
+    const float4 zv = z[i], rv = r[i];
+    a += (double)zv.x * rv.x + (double)zv.y * rv.y + (double)zv.z * rv.z + (double)zv.w * rv.w;
+    if (!init) {
+      const float4 qv = q[i];
+      b += (double)zv.x * qv.x + (double)zv.y * qv.y + (double)zv.z * qv.z + (double)zv.w * qv.w;
+    }
+  }
+  a = block_sum<256>(a, red);
+  b = block_sum<256>(b, red);
+  if (threadIdx.x == 0) {
+    partials[2 * blockIdx.x] = a;
+    partials[2 * blockIdx.x + 1] = b;
+  }
+  if (last_block(counter)) {
+    double ta = 0.0, tb = 0.0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += 256) {
+      ta += partials[2 * i];
+      tb += partials[2 * i + 1];
+    }
+    ta = block_sum<256>(ta, red);
+    tb = block_sum<256>(tb, red);
+    if (threadIdx.x == 0) {
+      if (init) {
+        st->rho = ta;
+        st->beta = 0.0;
+      } else {
+        st->beta = -st->alpha * tb / st->rho;
+        st->rho = ta;
+      }
+      if (!(ta == ta) || ta == 0.0) {
+        st->done = 3;
+        if (!(ta == ta)) st->status = -5;
+      }
+      *counter = 0;
+    }
+  }
+}
+
+// Standard normal samples at unknown cells (diag != 0) from a counter-based hash.
+__device__ __forceinline__ uint32_t mix32(uint32_t x) {
+  x ^= x >> 16; x *= 0x7feb352dU; x ^= x >> 15; x *= 0x846ca68bU; x ^= x >> 16;
+  return x;
+}
+__global__ void k_rand_unknowns(int n, const float *diag, uint32_t seed, float *e) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float v = 0.f;
+    if (diag[i] != 0.f) {
+      const uint32_t h1 = mix32((uint32_t)i * 2654435761u ^ seed), h2 = mix32(h1 ^ 0x9e3779b9u);
+      const float u1 = ((h1 >> 8) + 1) * (1.0f / 16777217.0f), u2 = (h2 >> 8) * (1.0f / 16777216.0f);
+      v = sqrtf(-2.f * logf(u1)) * cospif(2.f * u2);
+    }
+    e[i] = v;
+  }
+}
+__global__ void k_scale_f32(int n, float *a, float s) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] *= s;
+}
+__global__ void k_axpby_f32(int n, float a, const float *x, float b, float *y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = a * x[i] + b * y[i];
+}
+
+// ---------------------------------------------------------------------------
 // host launchers
 
 static int grid_for(long long n, int per, int cap) {
@@ -1127,5 +1200,27 @@ void launch_scale_f64_f32(int n, const double *a, double sc, float *b, cudaStrea
 void launch_scale_f32_f64(int n, const float *a, double sc, double *b, cudaStream_t s) {
   count_launches(1);
   k_scale_f32_f64<<<grid_for(n, 256 * 4, 148 * 8), 256, 0, s>>>(n, a, sc, b);
+}
+}  // namespace shkz
+
+namespace shkz {
+void launch_fpcg_dots(int n, const float *z, const float *r, const float *q, double *partials, unsigned *counter,
+                      SolverState *st, int init, cudaStream_t s) {
+  const int n4 = n / 4;
+  count_launches(1);
+  k_fpcg_dots<<<grid_for(n4, 256 * 4, 148 * 8), 256, 0, s>>>(n4, (const float4 *)z, (const float4 *)r,
+                                                               (const float4 *)q, partials, counter, st, init);
+}
+void launch_rand_unknowns(int n, const float *diag, unsigned seed, float *e, cudaStream_t s) {
+  count_launches(1);
+  k_rand_unknowns<<<grid_for(n, 256 * 4, 148 * 8), 256, 0, s>>>(n, diag, seed, e);
+}
+void launch_scale_f32(int n, float *a, float sc, cudaStream_t s) {
+  count_launches(1);
+  k_scale_f32<<<grid_for(n, 256 * 4, 148 * 8), 256, 0, s>>>(n, a, sc);
+}
+void launch_axpby_f32(int n, float a, const float *x, float b, float *y, cudaStream_t s) {
+  count_launches(1);
+  k_axpby_f32<<<grid_for(n, 256 * 4, 148 * 8), 256, 0, s>>>(n, a, x, b, y);
 }
 }  // namespace shkz

@@ -40,4 +40,10 @@ void launch_xpby64(int n, const double *x, double beta, double *y, cudaStream_t 
 void launch_scale_f64_f32(int n, const double *a, double sc, float *b, cudaStream_t s);
 void launch_scale_f32_f64(int n, const float *a, double sc, double *b, cudaStream_t s);
 
+void launch_fpcg_dots(int n, const float *z, const float *r, const float *q, double *partials, unsigned *counter,
+                      SolverState *st, int init, cudaStream_t s);
+void launch_rand_unknowns(int n, const float *diag, unsigned seed, float *e, cudaStream_t s);
+void launch_scale_f32(int n, float *a, float sc, cudaStream_t s);
+void launch_axpby_f32(int n, float a, const float *x, float b, float *y, cudaStream_t s);
+
 }  // namespace shkz

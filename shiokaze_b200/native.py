@@ -75,6 +75,10 @@ EXPORTS = [
     "shkz_b200_errstr", "shkz_b200_last_error", "shkz_b200_project_host", "shkz_b200_project_device",
     "shkz_b200_stream", "shkz_b200_solve_csr", "shkz_b200_inspect", "shkz_b200_apply_preconditioner",
     "shkz_b200_apply_matrix", "shkz_b200_time_kernel",
+    "shkz_b200_learned_init", "shkz_b200_learned_param_count", "shkz_b200_learned_set_params",
+    "shkz_b200_learned_get_params", "shkz_b200_learned_apply", "shkz_b200_learned_dims",
+    "shkz_b200_learned_tensor", "shkz_b200_learned_backward", "shkz_b200_learned_train",
+    "shkz_b200_learned_save", "shkz_b200_learned_load", "shkz_b200_conv3d",
 ]
 
 _lib = None
@@ -108,6 +112,19 @@ def load(path: str = LIB_PATH):
     L.shkz_b200_apply_matrix.argtypes = [P, P, P]
     L.shkz_b200_time_kernel.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                         ctypes.POINTER(ctypes.c_longlong)]
+    L.shkz_b200_learned_init.argtypes = [P, ctypes.c_uint]
+    L.shkz_b200_learned_param_count.argtypes = [P]
+    L.shkz_b200_learned_param_count.restype = ctypes.c_longlong
+    L.shkz_b200_learned_set_params.argtypes = [P, P, ctypes.c_size_t]
+    L.shkz_b200_learned_get_params.argtypes = [P, P, ctypes.c_size_t, ctypes.c_int]
+    L.shkz_b200_learned_apply.argtypes = [P, P, P]
+    L.shkz_b200_learned_dims.argtypes = [P, P]
+    L.shkz_b200_learned_tensor.argtypes = [P, ctypes.c_int, P, ctypes.c_size_t, P]
+    L.shkz_b200_learned_backward.argtypes = [P, P, ctypes.c_size_t]
+    L.shkz_b200_learned_train.argtypes = [P, ctypes.c_int, ctypes.c_double, ctypes.c_uint, P]
+    L.shkz_b200_learned_save.argtypes = [P, ctypes.c_char_p]
+    L.shkz_b200_learned_load.argtypes = [P, ctypes.c_char_p]
+    L.shkz_b200_conv3d.argtypes = [ctypes.c_int] * 7 + [P, P, P, P, ctypes.c_int, P]
     _lib = L
     return L
 

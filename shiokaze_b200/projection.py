@@ -165,6 +165,70 @@ class MacPressureSolver3:
         self.context.check(rc, "shkz_b200_apply_preconditioner")
         return z
 
+    # -- learned preconditioner ------------------------------------------
+    def learned_init(self, seed: int = 0) -> None:
+        self.context.check(native.load().shkz_b200_learned_init(self.context.handle, seed), "learned_init")
+
+    def learned_params(self, gradients: bool = False) -> np.ndarray:
+        L = native.load()
+        n = L.shkz_b200_learned_param_count(self.context.handle)
+        out = np.zeros(n, np.float32)
+        self.context.check(L.shkz_b200_learned_get_params(self.context.handle, out.ctypes.data, n, int(gradients)),
+                           "learned_get_params")
+        return out
+
+    def learned_set_params(self, blob: np.ndarray) -> None:
+        blob = np.ascontiguousarray(blob, np.float32)
+        self.context.check(native.load().shkz_b200_learned_set_params(self.context.handle, blob.ctypes.data, blob.size),
+                           "learned_set_params")
+
+    def learned_apply(self, r: np.ndarray) -> np.ndarray:
+        r = np.ascontiguousarray(r, np.float32)
+        z = np.zeros_like(r)
+        self.context.check(native.load().shkz_b200_learned_apply(self.context.handle, r.ctypes.data, z.ctypes.data),
+                           "learned_apply")
+        return z
+
+    def learned_dims(self):
+        d = (ctypes.c_int * 3)()
+        self.context.check(native.load().shkz_b200_learned_dims(self.context.handle, d), "learned_dims")
+        return tuple(d)
+
+    TENSORS = ["X0", "A1", "S1", "P1", "A2", "S2", "P2", "A3", "B3", "C2", "D2", "C1", "D1", "Z"]
+
+    def learned_tensor(self, which, grad: bool = False) -> np.ndarray:
+        """Stored activation of the last network application (name or index);
+        "Z" is the raw output; grad=True gives the gradient w.r.t. the tensor."""
+        if isinstance(which, str):
+            which = self.TENSORS.index(which)
+        if grad:
+            which += 14
+        L = native.load()
+        shp = (ctypes.c_int * 4)()
+        self.context.check(L.shkz_b200_learned_tensor(self.context.handle, which, None, 0, shp), "learned_tensor")
+        out = np.zeros(tuple(shp), np.float32)
+        self.context.check(L.shkz_b200_learned_tensor(self.context.handle, which, out.ctypes.data, out.size, shp),
+                           "learned_tensor")
+        return out[..., 0] if which == 13 else out
+
+    def learned_backward(self, gZ: np.ndarray) -> np.ndarray:
+        gZ = np.ascontiguousarray(gZ, np.float32)
+        self.context.check(native.load().shkz_b200_learned_backward(self.context.handle, gZ.ctypes.data, gZ.size),
+                           "learned_backward")
+        return self.learned_params(gradients=True)
+
+    def learned_train(self, steps: int, lr: float = 1e-3, seed: int = 0) -> np.ndarray:
+        losses = np.zeros(max(1, steps), np.float64)
+        self.context.check(native.load().shkz_b200_learned_train(self.context.handle, steps, lr, seed,
+                                                                 losses.ctypes.data), "learned_train")
+        return losses[:steps]
+
+    def learned_save(self, path: str) -> None:
+        self.context.check(native.load().shkz_b200_learned_save(self.context.handle, path.encode()), "learned_save")
+
+    def learned_load(self, path: str) -> None:
+        self.context.check(native.load().shkz_b200_learned_load(self.context.handle, path.encode()), "learned_load")
+
     def apply_matrix(self, x: np.ndarray) -> np.ndarray:
         x = np.ascontiguousarray(x, np.float32)
         y = np.zeros_like(x)
