@@ -209,6 +209,26 @@ int shkz_b200_learned_save(shkz_b200_ctx *ctx, const char *path);
  * cout <= 128, even grid sizes. No reference counterpart. */
 int shkz_b200_conv3d(int nx, int ny, int nz, int c0, int c1, int cout, int planes, const float *in0,
                      const float *in1, const float *w, const float *bias, int relu, float *out);
+
+/* The same convolution for callers that cannot allocate device memory (for
+ * example an application that has reserved the whole GPU for its own pool
+ * allocator, or a time-critical loop that must not pay the device-wide
+ * synchronisation cudaMalloc/cudaFree may imply). It allocates nothing: all
+ * pointers are DEVICE arrays the caller owns -- in0 (nz,ny,nx,c0) and in1
+ * (nz/2,ny/2,nx/2,c1) BF16 bit patterns channels-last, w[27][cout][c0+c1]
+ * FP32, bias[cout] FP32 (may be NULL), out (nz,ny,nx,cout) BF16 bit patterns
+ * -- and `stream` is a cudaStream_t (NULL = the default stream); the call
+ * returns after the stream has drained. Its scratch (packed weights, block
+ * flags, an error word) is a fixed 1.1 MiB array in the library that each GPU
+ * holds until exit. Limits: cout in {16, 32, 64, 128}, c0 + c1 <= 128 (both
+ * multiples of 16), at most 2^18 output blocks of 8x16x8 voxels (a 512^3 grid);
+ * larger sizes return SHKZ_B200_ERR_LIMIT. The first call on a device (with
+ * that device current) looks up the array's device address; make it before
+ * any stream capture. Calls share the array, so calls that overlap on the GPU
+ * race: serialise them. No counterpart in the reference. */
+int shkz_b200_conv3d_noalloc(int nx, int ny, int nz, int c0, int c1, int cout, int planes, const uint16_t *in0,
+                             const uint16_t *in1, const float *w, const float *bias, int relu, uint16_t *out,
+                             void *stream);
 int shkz_b200_learned_load(shkz_b200_ctx *ctx, const char *path);
 
 #ifdef __cplusplus

@@ -28,8 +28,9 @@ UNITS = {
     "solver.cu": [],
     "learned.cu": [],
     "api.cu": [],
+    "noalloc.cu": [],
 }
-HEADERS = ["common.cuh", "kernels.h", "solver.h", "learned.h"]
+HEADERS = ["common.cuh", "kernels.h", "solver.h", "learned.h", "tc_conv.cuh"]
 
 
 def _stale(target: str, deps) -> bool:

@@ -975,6 +975,47 @@ int conv3d_run(int nx, int ny, int nz, int c0, int c1, int cout, int planes, con
   return rc;
 }
 
+__global__ void k_fill_u8(uint8_t *a, int n, uint8_t v) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = v;
+}
+
+// The same convolution on device arrays with caller-provided scratch (packed
+// weights, block activity, error word); launches on `s` and returns without
+// synchronising. cout must be 16, 32, 64 or 128 (output stride = cout).
+int conv3d_launch_scratch(int nx, int ny, int nz, int c0, int c1, int cout, int planes, const __nv_bfloat16 *in0,
+                          const __nv_bfloat16 *in1, const float *w, const float *bias, int relu, __nv_bfloat16 *out,
+                          __nv_bfloat16 *wpk, uint8_t *act, int *err, cudaStream_t s) {
+  const int cin = c0 + c1;
+  const int gbx = (nx + 7) / 8, gby = (ny + 15) / 16, gbz = (nz + 7) / 8;
+  const int nb = gbx * gby * gbz;
+  count_launches(3);
+  k_pack_weights<<<256, 256, 0, s>>>(w, cout, cin, cout, cin, 0, wpk);
+  k_fill_u8<<<grid_blocks((size_t)nb, 256, 1024), 256, 0, s>>>(act, nb, 1);
+  if (cudaMemsetAsync(err, 0, sizeof(int), s) != cudaSuccess) return SHKZ_B200_ERR_CUDA;
+  ConvArgs a;
+  a.in0 = in0;
+  a.in1 = c1 ? in1 : nullptr;
+  a.c0 = c0;
+  a.c1 = c1;
+  a.nx = nx; a.ny = ny; a.nz = nz;
+  a.hx = nx / 2; a.hy = ny / 2; a.hz = nz / 2;
+  a.wpk = wpk;
+  a.bias = bias;
+  a.bias_n = cout;
+  a.cout = cout;
+  a.relu = relu;
+  a.out = out;
+  a.out32 = nullptr;
+  a.block_act = act;
+  a.gbx = gbx; a.gby = gby; a.gbz = gbz;
+  a.planes = planes;
+  a.err = err;
+  if (cudaFuncSetAttribute(k_conv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess)
+    return SHKZ_B200_ERR_CUDA;
+  k_conv_tc<<<nb * (8 / planes), 128, conv_smem_bytes(planes, cout), s>>>(a);
+  return cudaGetLastError() == cudaSuccess ? 0 : SHKZ_B200_ERR_CUDA;
+}
+
 // ---------------------------------------------------------------------------
 // entry points used by the context (api.cu)
 

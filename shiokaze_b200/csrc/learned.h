@@ -2,6 +2,7 @@
 #pragma once
 #include "common.cuh"
 #include "kernels.h"
+#include <cuda_bf16.h>
 #include "../../include/shkz_b200.h"
 
 namespace shkz {
@@ -39,6 +40,9 @@ size_t learned_tensor_size(const LearnedModel *m, int t);
 void learned_tensor_shape(const LearnedModel *m, int t, int *shape4);
 int learned_tensor_dense(LearnedModel *m, int t, float *out, cudaStream_t s);
 int learned_grad_dense(LearnedModel *m, int t, float *out, cudaStream_t s);
+int conv3d_launch_scratch(int nx, int ny, int nz, int c0, int c1, int cout, int planes, const __nv_bfloat16 *in0,
+                          const __nv_bfloat16 *in1, const float *w, const float *bias, int relu, __nv_bfloat16 *out,
+                          __nv_bfloat16 *wpk, uint8_t *act, int *err, cudaStream_t s);
 int conv3d_run(int nx, int ny, int nz, int c0, int c1, int cout, int planes, const float *in0_h, const float *in1_h,
                const float *w_h, const float *bias_h, int relu, float *out_h);
 }  // namespace shkz

@@ -78,7 +78,7 @@ EXPORTS = [
     "shkz_b200_learned_init", "shkz_b200_learned_param_count", "shkz_b200_learned_set_params",
     "shkz_b200_learned_get_params", "shkz_b200_learned_apply", "shkz_b200_learned_dims",
     "shkz_b200_learned_tensor", "shkz_b200_learned_backward", "shkz_b200_learned_train",
-    "shkz_b200_learned_save", "shkz_b200_learned_load", "shkz_b200_conv3d",
+    "shkz_b200_learned_save", "shkz_b200_learned_load", "shkz_b200_conv3d", "shkz_b200_conv3d_noalloc",
 ]
 
 _lib = None
@@ -125,6 +125,7 @@ def load(path: str = LIB_PATH):
     L.shkz_b200_learned_save.argtypes = [P, ctypes.c_char_p]
     L.shkz_b200_learned_load.argtypes = [P, ctypes.c_char_p]
     L.shkz_b200_conv3d.argtypes = [ctypes.c_int] * 7 + [P, P, P, P, ctypes.c_int, P]
+    L.shkz_b200_conv3d_noalloc.argtypes = [ctypes.c_int] * 7 + [P, P, P, P, ctypes.c_int, P, P]
     _lib = L
     return L
 
