@@ -34,6 +34,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+DEFAULT_MODEL = os.path.join(ROOT, "shiokaze_b200", "models", "shkz_net.bin")
 METRIC = "ms/projection & PCG iters to 1e-6 rel. residual at 256³: learned vs plain, 1 B200"
 UNIT = "ms/projection"
 
@@ -194,6 +195,9 @@ def main():
     ap.add_argument("--precond", default="mic0", choices=["mic0", "none", "learned"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--mic-block", type=int, default=16, choices=[8, 16],
+                    help="MIC(0) sweep block edge (16: 2x2x2 tiles per CTA)")
+    ap.add_argument("--model", default=None, help="trained network for --precond learned")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -220,8 +224,12 @@ def main():
     cfg.preconditioner = {"mic0": native.PRECOND_MIC0, "none": native.PRECOND_NONE,
                           "learned": native.PRECOND_LEARNED}[args.precond]
     cfg.device = local
+    cfg.mic_block = args.mic_block
     ctx = native.Context(cfg)
     L = native.load()
+    if args.precond == "learned":
+        model = args.model or DEFAULT_MODEL
+        ctx.check(L.shkz_b200_learned_load(ctx.handle, model.encode()), "shkz_b200_learned_load")
     stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
 
     # device-resident inputs

@@ -78,7 +78,8 @@ typedef struct shkz_b200_config {
   int check_interval;         /* iterations per device-side batch between host checks (default 16) */
   int stall_window;           /* learned FPCG: iterations without progress before MIC(0) fallback */
   int device;                 /* CUDA device ordinal (default 0) */
-  int reserved[8];
+  int mic_block;              /* MIC(0) sweep block edge: 16 (default, 2x2x2 tiles per CTA) or 8 */
+  int reserved[7];
 } shkz_b200_config;
 
 /* Fill *cfg with the defaults listed above. */

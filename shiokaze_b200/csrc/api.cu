@@ -60,12 +60,17 @@ struct shkz_b200_ctx {
   SolverState *st = nullptr;
   int *wflags = nullptr;  // factor wavefront flags [cap_pool]
   unsigned long long *faces_f = nullptr, *faces_b = nullptr;  // [cap_pool][3][64] epoch-tagged sweep faces
+  // 16^3 macro tiles of the MIC(0) sweeps
+  int KM = 0, cap_macro = 0;
+  int *mcount = nullptr, *mstate = nullptr, *mtile = nullptr, *mnbr = nullptr, *msched = nullptr, *msub = nullptr;
+  unsigned long long *mfaces_f = nullptr, *mfaces_b = nullptr;  // [cap_macro][3][256]
   void *ws = nullptr;     // 3 WaveSync
   // last projection
   Geometry G{};
   int K = 0;
   long long unknowns = 0;
   int has_system = 0;
+  int mic_ready = 0;  // d32 holds the MIC(0) factor of the current system
   LearnedModel *model = nullptr;
   int model_ready = 0;  // block activity computed for the current system
   AssemblyInputs last_in{};
@@ -89,6 +94,7 @@ extern "C" void shkz_b200_default_config(shkz_b200_config *c) {
   c->check_interval = 16;
   c->stall_window = 8;
   c->device = 0;
+  c->mic_block = 16;
 }
 
 extern "C" const char *shkz_b200_errstr(int code) {
@@ -152,6 +158,8 @@ static int ensure_grid(shkz_b200_ctx *ctx, const Geometry &G) {
     GROW(tile_count, G.ntiles);
     GROW(tile_state, G.ntiles);
     GROW(bsum, (G.ntiles + 1023) / 1024 + 1);
+    GROW(mcount, G.ntiles);
+    GROW(mstate, G.ntiles);
     ctx->cap_tiles = G.ntiles;
   }
   if (!ctx->level_count) {
@@ -209,10 +217,58 @@ static int ensure_pool(shkz_b200_ctx *ctx, int K) {
   SHKZ_CUDA_TRY(cudaMemsetAsync(ctx->faces_f, 0, sizeof(unsigned long long) * (size_t)cap * 3 * 64, ctx->stream));
   SHKZ_CUDA_TRY(cudaMemsetAsync(ctx->faces_b, 0, sizeof(unsigned long long) * (size_t)cap * 3 * 64, ctx->stream));
   if (ctx->ws) {
-    // flags were reset: restart the epochs
+    // flags were reset: restart the epochs (macro faces too, so no stale tag matches)
     SHKZ_CUDA_TRY(cudaMemsetAsync(ctx->ws, 0, 3 * wave_sync_bytes(), ctx->stream));
+    if (ctx->mfaces_f) {
+      SHKZ_CUDA_TRY(cudaMemsetAsync(ctx->mfaces_f, 0, sizeof(unsigned long long) * (size_t)ctx->cap_macro * 768,
+                                    ctx->stream));
+      SHKZ_CUDA_TRY(cudaMemsetAsync(ctx->mfaces_b, 0, sizeof(unsigned long long) * (size_t)ctx->cap_macro * 768,
+                                    ctx->stream));
+    }
   }
   ctx->cap_pool = cap;
+  return 0;
+}
+
+static int ensure_macro(shkz_b200_ctx *ctx, int KM) {
+  if (KM <= ctx->cap_macro) return 0;
+  const int cap = KM + KM / 4 + 16;
+  GROW(mtile, cap);
+  GROW(mnbr, (size_t)cap * 6);
+  GROW(msched, cap);
+  GROW(msub, (size_t)cap * 8);
+  GROW(mfaces_f, (size_t)cap * 768);
+  GROW(mfaces_b, (size_t)cap * 768);
+  // new face words carry epoch 0, which no sweep uses
+  SHKZ_CUDA_TRY(cudaMemsetAsync(ctx->mfaces_f, 0, sizeof(unsigned long long) * (size_t)cap * 768, ctx->stream));
+  SHKZ_CUDA_TRY(cudaMemsetAsync(ctx->mfaces_b, 0, sizeof(unsigned long long) * (size_t)cap * 768, ctx->stream));
+  ctx->cap_macro = cap;
+  return 0;
+}
+
+// 16^3 macro tiles over the pool (2x2x2 tiles each) for the MIC(0) sweeps:
+// the pool kernels run again on a grid twice as coarse, with the summed
+// unknown counts of each macro tile's eight tiles.
+static int build_macro_tiles(shkz_b200_ctx *ctx, const Geometry &G, int K, cudaStream_t s) {
+  ctx->KM = 0;
+  if (K <= 0 || ctx->cfg.mic_block == 8) return 0;
+  Geometry M = G;
+  M.bx = (G.bx + 1) / 2;
+  M.by = (G.by + 1) / 2;
+  M.bz = (G.bz + 1) / 2;
+  M.ntiles = (long long)M.bx * M.by * M.bz;
+  launch_macro_count(G, ctx->tile_count, M, ctx->mcount, s);
+  const int KM = pool_count(M, ctx->mcount, ctx->bsum, ctx->total, s);
+  if (KM < 0) {
+    shkz_set_cuda_error(cudaGetLastError(), "pool_count (macro)", __FILE__, __LINE__);
+    return SHKZ_B200_ERR_CUDA;
+  }
+  int rc = ensure_macro(ctx, KM > 0 ? KM : 1);
+  if (rc) return rc;
+  build_macro(G, M, ctx->tile_count, ctx->tile_state, ctx->mcount, ctx->mstate, ctx->mtile, ctx->mnbr,
+              ctx->level_count, ctx->msched, ctx->msub, KM, ctx->bsum, s);
+  SHKZ_CUDA_TRY(cudaGetLastError());
+  ctx->KM = KM;
   return 0;
 }
 
@@ -271,7 +327,8 @@ extern "C" void shkz_b200_destroy(shkz_b200_ctx *ctx) {
                   ctx->offz64, ctx->rhs64, ctx->colsum, ctx->dmic64, ctx->x64, ctx->r64, ctx->xref64, ctx->p64, ctx->q64,
                   ctx->z64, ctx->x, ctx->r,
                   ctx->p, ctx->q, ctx->z, ctx->t, ctx->p32, ctx->partials, ctx->out4, ctx->counter, ctx->st,
-                  ctx->wflags, ctx->faces_f, ctx->faces_b, ctx->ws, ctx->st_scratch};
+                  ctx->wflags, ctx->faces_f, ctx->faces_b, ctx->ws, ctx->st_scratch, ctx->mcount, ctx->mstate,
+                  ctx->mtile, ctx->mnbr, ctx->msched, ctx->msub, ctx->mfaces_f, ctx->mfaces_b};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (ctx->model) learned_free(ctx->model);
@@ -294,6 +351,12 @@ static PoolSystem pool_system(shkz_b200_ctx *ctx) {
   S.K = ctx->K;
   S.nbr = ctx->nbr;
   S.sched = ctx->sched;
+  S.KM = ctx->cfg.mic_block == 8 ? 0 : ctx->KM;
+  S.msched = ctx->msched;
+  S.mnbr = ctx->mnbr;
+  S.msub = ctx->msub;
+  S.mfaces_f = ctx->mfaces_f;
+  S.mfaces_b = ctx->mfaces_b;
   S.diag = ctx->diag;
   S.offx = ctx->offx;
   S.offy = ctx->offy;
@@ -339,7 +402,7 @@ static void launch_iteration_tail(shkz_b200_ctx *ctx, const PoolSystem &S, int n
   if (precond == SHKZ_B200_PRECOND_MIC0) {
     launch_mic_apply(S, ctx->d32, ctx->r, ctx->t, ctx->z, ctx->partials, ctx->faces_f,
                      ctx->faces_b, wsync(ctx, 1), wsync(ctx, 2), ctx->st, s);
-    launch_finish_rho(ctx->partials, ctx->K, ctx->st, 0, s);
+    launch_finish_rho(ctx->partials, mic_partial_count(S), ctx->st, 0, s);
     launch_update_p(n, ctx->z, ctx->p, ctx->st, s);
   } else {
     launch_finish_rho_r2(ctx->st, 0, s);
@@ -378,7 +441,7 @@ static int solve_system(shkz_b200_ctx *ctx, double tol, int precond, shkz_b200_r
   if (precond == SHKZ_B200_PRECOND_MIC0) {
     launch_mic_apply(S, ctx->d32, ctx->r, ctx->t, ctx->z, ctx->partials, ctx->faces_f,
                      ctx->faces_b, wsync(ctx, 1), wsync(ctx, 2), ctx->st, s);
-    launch_finish_rho(ctx->partials, ctx->K, ctx->st, 1, s);
+    launch_finish_rho(ctx->partials, mic_partial_count(S), ctx->st, 1, s);
     SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->p, ctx->z, sizeof(float) * n, cudaMemcpyDeviceToDevice, s));
   } else {
     launch_finish_rho_r2(ctx->st, 1, s);
@@ -560,6 +623,8 @@ static int project_device(shkz_b200_ctx *ctx, const shkz_b200_project_args *a, s
   pool_assign(G, ctx->tile_count, K, ctx->bsum, ctx->tile_state, ctx->pool_tile, ctx->nbr, ctx->level_count,
               ctx->sched, s);
   SHKZ_CUDA_TRY(cudaGetLastError());
+  rc = build_macro_tiles(ctx, G, K, s);
+  if (rc) return rc;
   ctx->K = K;
   ctx->G = G;
   ctx->model_ready = 0;
@@ -569,9 +634,12 @@ static int project_device(shkz_b200_ctx *ctx, const shkz_b200_project_args *a, s
   launch_coeff(in, ctx->flags, ctx->pool_tile, K, ctx->unk, co, s);
   const int precond = ctx->cfg.preconditioner;
   const PoolSystem S = pool_system(ctx);
-  if (K > 0 && (precond == SHKZ_B200_PRECOND_MIC0 || precond == SHKZ_B200_PRECOND_LEARNED))
+  ctx->mic_ready = 0;
+  if (K > 0 && (precond == SHKZ_B200_PRECOND_MIC0 || precond == SHKZ_B200_PRECOND_LEARNED)) {
     launch_mic_factor(S, ctx->colsum, ctx->cfg.mic_omega, ctx->cfg.mic_min_diag_ratio, ctx->dmic64, ctx->d32,
                       ctx->wflags, wsync(ctx, 0), s);
+    ctx->mic_ready = 1;
+  }
   SHKZ_CUDA_TRY(cudaGetLastError());
   cudaEventRecord(ctx->ev[1], s);
   ctx->has_system = 1;
@@ -1044,7 +1112,7 @@ static int learned_solve(shkz_b200_ctx *ctx, double tol, shkz_b200_result *res) 
     return learned_apply(ctx->model, LS, ctx->r, rmax_scaled, ctx->z, s);
   };
   if ((rc = precondition(1.0))) return rc;
-  launch_fpcg_dots(n, ctx->z, ctx->r, ctx->q, ctx->partials, ctx->counter + 5, ctx->st, 1, s);
+  launch_fpcg_dots(n, ctx->z, ctx->r, ctx->q, ctx->partials, ctx->counter + 5, ctx->st, 1 | 2, s);
   SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->p, ctx->z, sizeof(float) * n, cudaMemcpyDeviceToDevice, s));
   const int max_it = ctx->cfg.max_iterations;
   const int W = ctx->cfg.stall_window > 0 ? ctx->cfg.stall_window : 8;
@@ -1057,6 +1125,17 @@ static int learned_solve(shkz_b200_ctx *ctx, double tol, shkz_b200_result *res) 
     launch_update_xr(n, ctx->p, ctx->q, ctx->x, ctx->r, ctx->partials, ctx->counter + 1, ctx->st, max_it, s);
     SHKZ_CUDA_TRY(cudaMemcpyAsync(&hst, ctx->st, sizeof(hst), cudaMemcpyDeviceToHost, s));
     SHKZ_CUDA_TRY(cudaStreamSynchronize(s));
+    if (hst.done == 5) {
+      // the learned z broke down (z.r <= 0 or not finite): x and r are those of
+      // the last completed iteration; continue with MIC(0) from r
+      use_mic = true;
+      res->fallbacks += 1;
+      launch_state_resume(ctx->st, hst.ru_threshold, s);
+      if ((rc = precondition(hst.rmax))) break;
+      launch_fpcg_dots(n, ctx->z, ctx->r, ctx->q, ctx->partials, ctx->counter + 5, ctx->st, 1, s);
+      SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->p, ctx->z, sizeof(float) * n, cudaMemcpyDeviceToDevice, s));
+      continue;
+    }
     if (hst.done == 3 || hst.status == -5) { rc = SHKZ_B200_ERR_NAN; break; }
     if (hst.done == 2) break;
     true_checked = false;
@@ -1085,7 +1164,8 @@ static int learned_solve(shkz_b200_ctx *ctx, double tol, shkz_b200_result *res) 
       restart = true;
     }
     if ((rc = precondition(rmax))) break;
-    launch_fpcg_dots(n, ctx->z, ctx->r, ctx->q, ctx->partials, ctx->counter + 5, ctx->st, restart ? 1 : 0, s);
+    launch_fpcg_dots(n, ctx->z, ctx->r, ctx->q, ctx->partials, ctx->counter + 5, ctx->st,
+                     (restart ? 1 : 0) | (use_mic ? 0 : 2), s);
     if (restart) SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->p, ctx->z, sizeof(float) * n, cudaMemcpyDeviceToDevice, s));
     else launch_update_p(n, ctx->z, ctx->p, ctx->st, s);
   }
@@ -1243,6 +1323,13 @@ extern "C" int shkz_b200_learned_train(shkz_b200_ctx *ctx, int steps, double lr,
   const PoolSystem S = pool_system(ctx);
   const LearnedSystem LS = learned_system(ctx);
   const int n = ctx->K * SHKZ_TC;
+  if (!ctx->mic_ready) {
+    launch_mic_factor(S, ctx->colsum, ctx->cfg.mic_omega, ctx->cfg.mic_min_diag_ratio, ctx->dmic64, ctx->d32,
+                      ctx->wflags, wsync(ctx, 0), s);
+    ctx->mic_ready = 1;
+  }
+  const int np = mic_partial_count(S);
+  std::vector<double> hp((size_t)np);
   for (int i = 0; i < steps; ++i) {
     const int kind = i % 3;
     // r (FP32 pool) in ctx->r; scratch: ctx->t (noise), ctx->q (A e)
@@ -1267,8 +1354,18 @@ extern "C" int shkz_b200_learned_train(shkz_b200_ctx *ctx, int steps, double lr,
     SHKZ_CUDA_TRY(cudaMemcpyAsync(&a3, ctx->st_scratch, sizeof(a3), cudaMemcpyDeviceToHost, s));
     SHKZ_CUDA_TRY(cudaStreamSynchronize(s));
     if (a3.rmax0 > 0) launch_scale_f32(n, ctx->r, (float)(1.0 / a3.rmax0), s);
+    // loss scale: the MIC(0) energy 1/2 r.M^-1 r estimates 1/2 r.A^-1 r, so the
+    // normalised loss is near -1 at the optimum whatever the system and residual
+    launch_mic_apply(S, ctx->d32, ctx->r, ctx->t, ctx->z, ctx->partials, ctx->faces_f, ctx->faces_b, wsync(ctx, 1),
+                     wsync(ctx, 2), nullptr, s);
+    SHKZ_CUDA_TRY(cudaMemcpyAsync(hp.data(), ctx->partials, sizeof(double) * np, cudaMemcpyDeviceToHost, s));
+    SHKZ_CUDA_TRY(cudaStreamSynchronize(s));
+    double rz = 0.0;
+    for (double v : hp) rz += v;
+    const double gscale = (rz > 0.0 && rz < 1e300) ? 2.0 / rz : 1.0;
     double loss = 0.0;
-    rc = learned_train_step(ctx->model, LS, S, ctx->r, ctx->z, ctx->q, ctx->partials, ctx->counter, (float)lr, &loss, s);
+    rc = learned_train_step(ctx->model, LS, S, ctx->r, ctx->z, ctx->q, ctx->partials, ctx->counter, (float)lr,
+                            gscale, &loss, s);
     if (rc) return rc;
     if (losses) losses[i] = loss;
   }

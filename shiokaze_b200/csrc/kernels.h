@@ -30,6 +30,12 @@ struct PoolSystem {
   const int *sched;      // [K] pool indices ordered by wavefront level
   const float *diag, *offx, *offy, *offz;
   const double *diag64, *offx64, *offy64, *offz64;
+  // 16^3 macro tiles (2x2x2 pool tiles) for the MIC(0) sweeps
+  int KM;
+  const int *msched;     // [KM] macro tiles ordered by wavefront level
+  const int *mnbr;       // [KM][6] neighbour macro tiles or -1
+  const int *msub;       // [KM][8] pool index of sub-tile (x + 2y + 4z) or -1
+  unsigned long long *mfaces_f, *mfaces_b;  // [KM][3][256] epoch-tagged sweep faces
 };
 
 // assemble.cu

@@ -502,8 +502,10 @@ __global__ void k_adam(float *w, const float *g, float *m, float *v, int n, floa
 
 // dL/dZ for the energy loss 1/2 z.A z - z.r (z, r scaled): q = A z - r at unknowns,
 // scattered into the dense FP32 gradient of the output; also the loss terms.
+// gradient gscale (A z - r) and energy gscale (1/2 z.Az - z.r) of the output
 __global__ void k_energy_grad(Geometry G, int NX, int NY, const int *pool_tile, int K, const uint8_t *unk,
-                              const float *Az, const float *zp, const float *rp, float *gZ, double *partials) {
+                              const float *Az, const float *zp, const float *rp, float gscale, float *gZ,
+                              double *partials) {
   __shared__ double red[8];
   double e = 0.0;
   const size_t n = (size_t)K * SHKZ_TC;
@@ -515,10 +517,10 @@ __global__ void k_energy_grad(Geometry G, int NX, int NY, const int *pool_tile, 
     if (x >= G.nx || y >= G.ny || z >= G.nz) continue;
     if (!unk[(size_t)x + (size_t)G.nx * ((size_t)y + (size_t)G.ny * z)]) continue;
     const float q = Az[o] - rp[o];
-    gZ[((size_t)z * NY + y) * NX + x] = q;
+    gZ[((size_t)z * NY + y) * NX + x] = gscale * q;
     e += 0.5 * (double)zp[o] * Az[o] - (double)zp[o] * rp[o];
   }
-  e = block_sum<256>(e, red);
+  e = block_sum<256>(e, red) * (double)gscale;
   if (threadIdx.x == 0) partials[blockIdx.x] = e;
 }
 
@@ -1085,8 +1087,8 @@ void learned_dense_dims(const LearnedModel *m, int *nx, int *ny, int *nz) {
 // gradient of the A-norm error 1/2 (z - A^-1 r).A (z - A^-1 r)), r scaled to
 // ||r||inf = 1. Az_pool and z_pool are scratch pool vectors.
 int learned_train_step(LearnedModel *m, const LearnedSystem &sys, const PoolSystem &S, const float *r_pool,
-                       float *z_pool, float *Az_pool, double *partials, unsigned *counter, float lr, double *loss,
-                       cudaStream_t s) {
+                       float *z_pool, float *Az_pool, double *partials, unsigned *counter, float lr, double gscale,
+                       double *loss, cudaStream_t s) {
   int rc = learned_apply(m, sys, r_pool, 1.0, z_pool, s);
   if (rc) return rc;
   launch_spmv(S, z_pool, Az_pool, partials, counter, nullptr, 1, s);
@@ -1094,7 +1096,7 @@ int learned_train_step(LearnedModel *m, const LearnedSystem &sys, const PoolSyst
   const int nb = 148 * 4;
   count_launches(1);
   k_energy_grad<<<nb, 256, 0, s>>>(sys.G, m->NX[0], m->NY[0], sys.pool_tile, sys.K, sys.unk, Az_pool, z_pool, r_pool,
-                                   m->gZ, m->partials);
+                                   (float)gscale, m->gZ, m->partials);
   std::vector<double> hp(nb);
   cudaMemcpyAsync(hp.data(), m->partials, sizeof(double) * nb, cudaMemcpyDeviceToHost, s);
   rc = backward(m, s);

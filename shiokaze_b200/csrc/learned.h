@@ -33,8 +33,8 @@ int learned_output_dense(LearnedModel *m, float *Z_dense_dev, cudaStream_t s);
 size_t learned_dense_cells(const LearnedModel *m);
 void learned_dense_dims(const LearnedModel *m, int *nx, int *ny, int *nz);
 int learned_train_step(LearnedModel *m, const LearnedSystem &sys, const PoolSystem &S, const float *r_pool,
-                       float *z_pool, float *Az_pool, double *partials, unsigned *counter, float lr, double *loss,
-                       cudaStream_t s);
+                       float *z_pool, float *Az_pool, double *partials, unsigned *counter, float lr, double gscale,
+                       double *loss, cudaStream_t s);
 int learned_error(LearnedModel *m);
 size_t learned_tensor_size(const LearnedModel *m, int t);
 void learned_tensor_shape(const LearnedModel *m, int t, int *shape4);

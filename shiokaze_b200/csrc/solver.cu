@@ -747,6 +747,216 @@ __global__ void __launch_bounds__(64) k_mic_backward(PoolSystem S, const int *sc
 }
 
 // ---------------------------------------------------------------------------
+// MIC(0) sweeps over 16^3 macro tiles (2x2x2 pool tiles per CTA).
+//
+// Same recurrences as the 8^3 kernels above, on four times as many cells per
+// CTA (256 threads, one per x-row of 16 cells, 46 in-tile diagonals): the
+// wavefront then crosses half as many tile levels, and the hand-off between
+// levels -- not the arithmetic -- is what bounds a sweep. Shared memory holds
+// the macro tile's six FP32 fields (96 KB); faces are 256 epoch-tagged words.
+
+#define MT 16
+#define MTC 4096
+
+// macro tile counts = sum of the counts of its (up to) eight tiles
+__global__ void k_macro_count(Geometry G, const int *tile_count, Geometry M, int *macro_count) {
+  const long long n = M.ntiles;
+  for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+    const int mi = (int)(m % M.bx), mj = (int)((m / M.bx) % M.by), mk = (int)(m / ((long long)M.bx * M.by));
+    int c = 0;
+    for (int s = 0; s < 8; ++s) {
+      const int ti = 2 * mi + (s & 1), tj = 2 * mj + ((s >> 1) & 1), tk = 2 * mk + (s >> 2);
+      if (ti < G.bx && tj < G.by && tk < G.bz) c += tile_count[(long long)ti + (long long)G.bx * ((long long)tj + (long long)G.by * tk)];
+    }
+    macro_count[m] = c;
+  }
+}
+
+__global__ void k_macro_sub(Geometry G, Geometry M, const int *macro_tile, int KM, const int *tile_state, int *msub) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= KM * 8) return;
+  const int pm = e >> 3, s = e & 7;
+  const long long m = macro_tile[pm];
+  const int mi = (int)(m % M.bx), mj = (int)((m / M.bx) % M.by), mk = (int)(m / ((long long)M.bx * M.by));
+  const int ti = 2 * mi + (s & 1), tj = 2 * mj + ((s >> 1) & 1), tk = 2 * mk + (s >> 2);
+  int pt = -1;
+  if (ti < G.bx && tj < G.by && tk < G.bz) pt = tile_state[(long long)ti + (long long)G.bx * ((long long)tj + (long long)G.by * tk)];
+  msub[e] = pt;
+}
+
+// Stage five pool fields of the macro tile's sub-tiles into shared memory
+// (index x + 16y + 256z); absent sub-tiles read as zero.
+__device__ __forceinline__ void macro_load5(const int *sub, const float *s0, const float *s1, const float *s2,
+                                            const float *s3, const float *s4, float *d0, float *d1, float *d2,
+                                            float *d3, float *d4) {
+  for (int e = threadIdx.x; e < 8 * 128; e += blockDim.x) {
+    const int v = e & 127, st = e >> 7;
+    const int pt = sub[st];
+    const int c = v * 4;
+    const int x = (c & 7) + (st & 1) * 8, y = ((c >> 3) & 7) + ((st >> 1) & 1) * 8, z = (c >> 6) + (st >> 2) * 8;
+    const int o = x + 16 * y + 256 * z;
+    float4 a0 = make_float4(0.f, 0.f, 0.f, 0.f), a1 = a0, a2 = a0, a3 = a0, a4 = a0;
+    if (pt >= 0) {
+      const size_t b = (size_t)pt * (SHKZ_TC / 4) + v;
+      a0 = reinterpret_cast<const float4 *>(s0)[b];
+      a1 = reinterpret_cast<const float4 *>(s1)[b];
+      a2 = reinterpret_cast<const float4 *>(s2)[b];
+      a3 = reinterpret_cast<const float4 *>(s3)[b];
+      a4 = reinterpret_cast<const float4 *>(s4)[b];
+    }
+    *reinterpret_cast<float4 *>(d0 + o) = a0;
+    *reinterpret_cast<float4 *>(d1 + o) = a1;
+    *reinterpret_cast<float4 *>(d2 + o) = a2;
+    *reinterpret_cast<float4 *>(d3 + o) = a3;
+    *reinterpret_cast<float4 *>(d4 + o) = a4;
+  }
+}
+__device__ __forceinline__ void macro_store(const int *sub, const float *srcs, float *dst) {
+  for (int e = threadIdx.x; e < 8 * 128; e += blockDim.x) {
+    const int v = e & 127, st = e >> 7;
+    const int pt = sub[st];
+    if (pt < 0) continue;
+    const int c = v * 4;
+    const int x = (c & 7) + (st & 1) * 8, y = ((c >> 3) & 7) + ((st >> 1) & 1) * 8, z = (c >> 6) + (st >> 2) * 8;
+    reinterpret_cast<float4 *>(dst + (size_t)pt * SHKZ_TC)[v] = *reinterpret_cast<const float4 *>(srcs + x + 16 * y + 256 * z);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_mic_forward16(PoolSystem S, const float *__restrict__ d32,
+                                                       const float *__restrict__ r, float *__restrict__ t,
+                                                       unsigned long long *faces, WaveSync *ws, const SolverState *st) {
+  extern __shared__ __align__(16) float smf[];
+  float *T = smf, *R = T + MTC, *Dd = R + MTC, *WX = Dd + MTC, *WY = WX + MTC, *WZ = WY + MTC;
+  float *hx = WZ + MTC, *hy = hx + 256, *hz = hy + 256;
+  __shared__ int sub[8];
+  if (st && st->done) return;
+  int slot, epoch;
+  sweep_begin(ws, slot, epoch);
+  const int mt = S.msched[slot];
+  const int tid = threadIdx.x, jj = tid & 15, kk = tid >> 4;
+  if (tid < 8) sub[tid] = S.msub[mt * 8 + tid];
+  __syncthreads();
+  macro_load5(sub, r, d32, S.offx, S.offy, S.offz, R, Dd, WX, WY, WZ);
+  {
+    const int nxm = S.mnbr[mt * 6 + NB_XM], nym = S.mnbr[mt * 6 + NB_YM], nzm = S.mnbr[mt * 6 + NB_ZM];
+    bool ok = true;
+    hx[tid] = nxm >= 0 ? face_get(faces + ((size_t)nxm * 3 + 0) * 256 + tid, epoch, ok) : 0.0f;
+    hy[tid] = nym >= 0 ? face_get(faces + ((size_t)nym * 3 + 1) * 256 + tid, epoch, ok) : 0.0f;
+    hz[tid] = nzm >= 0 ? face_get(faces + ((size_t)nzm * 3 + 2) * 256 + tid, epoch, ok) : 0.0f;
+    if (!ok) atomicCAS(&ws->error, 0, slot + 1);
+  }
+  __syncthreads();
+  for (int s = 0; s < 3 * MT - 2; ++s) {
+    const int ii = s - jj - kk;
+    if (ii >= 0 && ii < MT) {
+      const int c = ii + MT * jj + MT * MT * kk;
+      const float tx = ii > 0 ? T[c - 1] : hx[jj + MT * kk];
+      const float ty = jj > 0 ? T[c - MT] : hy[ii + MT * kk];
+      const float tz = kk > 0 ? T[c - MT * MT] : hz[ii + MT * jj];
+      T[c] = Dd[c] * (R[c] + WX[c] * tx + WY[c] * ty + WZ[c] * tz);
+    }
+    __syncthreads();
+  }
+  {
+    unsigned long long *f = faces + (size_t)mt * 3 * 256;
+    const int u = tid & 15, v = tid >> 4;
+    face_put(f + 0 * 256 + tid, epoch, T[15 + MT * u + MT * MT * v]);
+    face_put(f + 1 * 256 + tid, epoch, T[u + MT * 15 + MT * MT * v]);
+    face_put(f + 2 * 256 + tid, epoch, T[u + MT * v + MT * MT * 15]);
+  }
+  macro_store(sub, T, t);
+  sweep_end(ws, epoch);
+}
+
+__global__ void __launch_bounds__(256) k_mic_backward16(PoolSystem S, const float *__restrict__ d32,
+                                                        const float *__restrict__ t, const float *__restrict__ r,
+                                                        float *__restrict__ z, double *partials,
+                                                        unsigned long long *faces, WaveSync *ws,
+                                                        const SolverState *st) {
+  extern __shared__ __align__(16) float smb[];
+  float *Z = smb, *Tt = Z + MTC, *Dd = Tt + MTC, *WX = Dd + MTC, *WY = WX + MTC, *WZ = WY + MTC;
+  float *hx = WZ + MTC, *hy = hx + 256, *hz = hy + 256, *ux = hz + 256, *uy = ux + 256, *uz = uy + 256;
+  __shared__ int sub[8];
+  __shared__ double red[8];
+  if (st && st->done) return;
+  int slot, epoch;
+  sweep_begin(ws, slot, epoch);
+  const int mt = S.msched[S.KM - 1 - slot];
+  const int tid = threadIdx.x, jj = tid & 15, kk = tid >> 4;
+  if (tid < 8) sub[tid] = S.msub[mt * 8 + tid];
+  __syncthreads();
+  macro_load5(sub, t, d32, S.offx, S.offy, S.offz, Tt, Dd, WX, WY, WZ);
+  const int nxp = S.mnbr[mt * 6 + NB_XP], nyp = S.mnbr[mt * 6 + NB_YP], nzp = S.mnbr[mt * 6 + NB_ZP];
+  {
+    // upper weights across the macro faces: lower weights of the +x/+y/+z
+    // macro neighbours' first column/row/plane, from their pool sub-tiles
+    const int u = tid & 15, v = tid >> 4;
+    float wxv = 0.f, wyv = 0.f, wzv = 0.f;
+    if (nxp >= 0) {  // cell (0, u, v) of the +x macro tile
+      const int pt = S.msub[nxp * 8 + 0 + 2 * (u >> 3) + 4 * (v >> 3)];
+      if (pt >= 0) wxv = S.offx[(size_t)pt * SHKZ_TC + 8 * (u & 7) + 64 * (v & 7)];
+    }
+    if (nyp >= 0) {  // cell (u, 0, v) of the +y macro tile
+      const int pt = S.msub[nyp * 8 + (u >> 3) + 4 * (v >> 3)];
+      if (pt >= 0) wyv = S.offy[(size_t)pt * SHKZ_TC + (u & 7) + 64 * (v & 7)];
+    }
+    if (nzp >= 0) {  // cell (u, v, 0) of the +z macro tile
+      const int pt = S.msub[nzp * 8 + (u >> 3) + 2 * (v >> 3)];
+      if (pt >= 0) wzv = S.offz[(size_t)pt * SHKZ_TC + (u & 7) + 8 * (v & 7)];
+    }
+    ux[tid] = wxv;
+    uy[tid] = wyv;
+    uz[tid] = wzv;
+    bool ok = true;
+    hx[tid] = nxp >= 0 ? face_get(faces + ((size_t)nxp * 3 + 0) * 256 + tid, epoch, ok) : 0.0f;
+    hy[tid] = nyp >= 0 ? face_get(faces + ((size_t)nyp * 3 + 1) * 256 + tid, epoch, ok) : 0.0f;
+    hz[tid] = nzp >= 0 ? face_get(faces + ((size_t)nzp * 3 + 2) * 256 + tid, epoch, ok) : 0.0f;
+    if (!ok) atomicCAS(&ws->error, 0, slot + 1);
+  }
+  __syncthreads();
+  for (int s = 3 * MT - 3; s >= 0; --s) {
+    const int ii = s - jj - kk;
+    if (ii >= 0 && ii < MT) {
+      const int c = ii + MT * jj + MT * MT * kk;
+      const float zx = ii < MT - 1 ? Z[c + 1] : hx[jj + MT * kk];
+      const float wx = ii < MT - 1 ? WX[c + 1] : ux[jj + MT * kk];
+      const float zy = jj < MT - 1 ? Z[c + MT] : hy[ii + MT * kk];
+      const float wy = jj < MT - 1 ? WY[c + MT] : uy[ii + MT * kk];
+      const float zz = kk < MT - 1 ? Z[c + MT * MT] : hz[ii + MT * jj];
+      const float wz = kk < MT - 1 ? WZ[c + MT * MT] : uz[ii + MT * jj];
+      Z[c] = Tt[c] + Dd[c] * (wx * zx + wy * zy + wz * zz);
+    }
+    __syncthreads();
+  }
+  {
+    unsigned long long *f = faces + (size_t)mt * 3 * 256;
+    const int u = tid & 15, v = tid >> 4;
+    face_put(f + 0 * 256 + tid, epoch, Z[MT * u + MT * MT * v]);
+    face_put(f + 1 * 256 + tid, epoch, Z[u + MT * MT * v]);
+    face_put(f + 2 * 256 + tid, epoch, Z[u + MT * v]);
+  }
+  macro_store(sub, Z, z);
+  // fused z.r over the macro tile's cells (absent sub-tiles contribute zero)
+  double dot = 0.0;
+  for (int e = tid; e < 8 * 128; e += 256) {
+    const int v = e & 127, stt = e >> 7;
+    const int pt = sub[stt];
+    if (pt < 0) continue;
+    const int c = v * 4;
+    const int x = (c & 7) + (stt & 1) * 8, y = ((c >> 3) & 7) + ((stt >> 1) & 1) * 8, zc = (c >> 6) + (stt >> 2) * 8;
+    const float4 zv = *reinterpret_cast<const float4 *>(Z + x + 16 * y + 256 * zc);
+    const float4 rv = reinterpret_cast<const float4 *>(r + (size_t)pt * SHKZ_TC)[v];
+    dot += (double)zv.x * rv.x + (double)zv.y * rv.y + (double)zv.z * rv.z + (double)zv.w * rv.w;
+  }
+  const double tot = block_sum<256>(dot, red);
+  if (tid == 0 && partials) partials[mt] = tot;
+  sweep_end(ws, epoch);
+}
+
+size_t mic16_smem_forward() { return sizeof(float) * (6 * MTC + 3 * 256); }
+size_t mic16_smem_backward() { return sizeof(float) * (6 * MTC + 6 * 256); }
+
+// ---------------------------------------------------------------------------
 // FP64 residual r64 = b64 - A64 x64 (x64 in FP64), its norms, and the FP32
 // scaled copy r32 = r64 / ||r64||inf for the next inner solve.
 __global__ void __launch_bounds__(256) k_residual64(PoolSystem S, const double *__restrict__ b, const double *__restrict__ x,
@@ -989,7 +1199,7 @@ __global__ void __launch_bounds__(256) k_fpcg_dots(int n4, const float4 *__restr
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += gridDim.x * blockDim.x) {
     const float4 zv = z[i], rv = r[i];
     a += (double)zv.x * rv.x + (double)zv.y * rv.y + (double)zv.z * rv.z + (double)zv.w * rv.w;
-    if (!init) {
+    if (!(init & 1)) {
       const float4 qv = q[i];
       b += (double)zv.x * qv.x + (double)zv.y * qv.y + (double)zv.z * qv.z + (double)zv.w * qv.w;
     }
@@ -1009,14 +1219,18 @@ __global__ void __launch_bounds__(256) k_fpcg_dots(int n4, const float4 *__restr
     ta = block_sum<256>(ta, red);
     tb = block_sum<256>(tb, red);
     if (threadIdx.x == 0) {
-      if (init) {
+      if (init & 1) {
         st->rho = ta;
         st->beta = 0.0;
       } else {
         st->beta = -st->alpha * tb / st->rho;
         st->rho = ta;
       }
-      if (!(ta == ta) || ta == 0.0) {
+      if (init & 2) {
+        // guarded (learned) preconditioner: z.r not positive and finite is a
+        // breakdown of the preconditioner, not of the solve (done = 5)
+        if (!(ta > 0.0) || !(tb == tb) || ta > 1e300) st->done = 5;
+      } else if (!(ta == ta) || ta == 0.0) {
         st->done = 3;
         if (!(ta == ta)) st->status = -5;
       }
@@ -1136,10 +1350,40 @@ void launch_mic_apply(const PoolSystem &S, const float *d32, const float *r, flo
                       unsigned long long *faces_f, unsigned long long *faces_b, void *ws_f, void *ws_b,
                       const SolverState *st, cudaStream_t s) {
   if (S.K <= 0) return;
+  if (S.KM > 0) {
+    static bool attr[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64 || !attr[dev]) {
+      cudaFuncSetAttribute(k_mic_forward16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mic16_smem_forward());
+      cudaFuncSetAttribute(k_mic_backward16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mic16_smem_backward());
+      if (dev >= 0 && dev < 64) attr[dev] = true;
+    }
+    count_launches(2);
+    k_mic_forward16<<<S.KM, 256, mic16_smem_forward(), s>>>(S, d32, r, t, S.mfaces_f, (WaveSync *)ws_f, st);
+    k_mic_backward16<<<S.KM, 256, mic16_smem_backward(), s>>>(S, d32, t, r, z, partials, S.mfaces_b,
+                                                               (WaveSync *)ws_b, st);
+    return;
+  }
   count_launches(1);
   k_mic_forward<<<S.K, 64, 0, s>>>(S, S.sched, d32, r, t, faces_f, (WaveSync *)ws_f, st);
   count_launches(1);
   k_mic_backward<<<S.K, 64, 0, s>>>(S, S.sched, d32, t, r, z, partials, faces_b, (WaveSync *)ws_b, st);
+}
+
+void build_macro(const Geometry &G, const Geometry &M, const int *tile_count, const int *tile_state, int *macro_count,
+                 int *macro_state, int *macro_tile, int *mnbr, int *level_count, int *msched, int *msub, int KM,
+                 const int *bsum, cudaStream_t s) {
+  pool_assign(M, macro_count, KM, bsum, macro_state, macro_tile, mnbr, level_count, msched, s);
+  if (KM > 0) {
+    count_launches(1);
+    k_macro_sub<<<(KM * 8 + 255) / 256, 256, 0, s>>>(G, M, macro_tile, KM, tile_state, msub);
+  }
+}
+
+void launch_macro_count(const Geometry &G, const int *tile_count, const Geometry &M, int *macro_count, cudaStream_t s) {
+  count_launches(1);
+  k_macro_count<<<grid_for(M.ntiles, 256, 148 * 8), 256, 0, s>>>(G, tile_count, M, macro_count);
 }
 
 void launch_residual64(const PoolSystem &S, const double *b, const double *x, double *r, double *partials,

@@ -40,6 +40,12 @@ void launch_xpby64(int n, const double *x, double beta, double *y, cudaStream_t 
 void launch_scale_f64_f32(int n, const double *a, double sc, float *b, cudaStream_t s);
 void launch_scale_f32_f64(int n, const float *a, double sc, double *b, cudaStream_t s);
 
+// partial sums written by one MIC(0) apply (one per CTA of the backward sweep)
+inline int mic_partial_count(const PoolSystem &S) { return S.KM > 0 ? S.KM : S.K; }
+void launch_macro_count(const Geometry &G, const int *tile_count, const Geometry &M, int *macro_count, cudaStream_t s);
+void build_macro(const Geometry &G, const Geometry &M, const int *tile_count, const int *tile_state, int *macro_count,
+                 int *macro_state, int *macro_tile, int *mnbr, int *level_count, int *msched, int *msub, int KM,
+                 const int *bsum, cudaStream_t s);
 void launch_fpcg_dots(int n, const float *z, const float *r, const float *q, double *partials, unsigned *counter,
                       SolverState *st, int init, cudaStream_t s);
 void launch_rand_unknowns(int n, const float *diag, unsigned seed, float *e, cudaStream_t s);

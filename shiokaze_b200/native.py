@@ -40,7 +40,8 @@ class Config(ctypes.Structure):
         ("check_interval", ctypes.c_int),
         ("stall_window", ctypes.c_int),
         ("device", ctypes.c_int),
-        ("reserved", ctypes.c_int * 8),
+        ("mic_block", ctypes.c_int),
+        ("reserved", ctypes.c_int * 7),
     ]
 
 

@@ -88,6 +88,7 @@ class MacPressureSolver3:
         c.check_interval = int(g("B200.CheckInterval", c.check_interval))
         c.stall_window = int(g("B200.StallWindow", c.stall_window))
         c.device = int(g("B200.Device", c.device))
+        c.mic_block = int(g("B200.MICBlock", c.mic_block))
         if self._ctx is not None:
             self._ctx.set_config(c)
 
