@@ -79,7 +79,11 @@ typedef struct shkz_b200_config {
   int stall_window;           /* learned FPCG: iterations without progress before MIC(0) fallback */
   int device;                 /* CUDA device ordinal (default 0) */
   int mic_block;              /* MIC(0) sweep block edge: 16 (default, 2x2x2 tiles per CTA) or 8 */
-  int reserved[7];
+  double gain;                /* Gain of the volume correction (default 1.0) */
+  int warm_start;             /* WarmStart (default 0) */
+  int index_tile;             /* tile edge of the caller's grids (TileSize, default 16): unknown numbering of
+                                 the warm-start vector */
+  int reserved[4];
 } shkz_b200_config;
 
 /* Fill *cfg with the defaults listed above. */
@@ -113,6 +117,8 @@ typedef struct shkz_b200_project_args {
   const float *solid_velocity[3];      /* faces, each may be NULL */
   float *pressure;                     /* cells, out, may be NULL */
   uint8_t *pressure_active;            /* cells, out, may be NULL */
+  double surface_tension;              /* surface_tension argument of project(); 0 = none */
+  const float *solid_density[3];       /* faces (set_solid_density), all NULL = none */
 } shkz_b200_project_args;
 
 typedef struct shkz_b200_result {
@@ -132,8 +138,25 @@ typedef struct shkz_b200_result {
   double ms_total;
   double ms_h2d, ms_d2h;     /* host paths only */
   long long kernel_launches; /* CUDA kernels this library launched for the call */
-  double reserved[7];
+  double volume_rhs_correct; /* volume correction added to every rhs row (record _volume_correct_rhs), else 0 */
+  double reserved[6];
 } shkz_b200_result;
+
+/* macproject3_interface::set_target_volume (macpressuresolver3.cpp:46-49):
+ * with Gain != 0 and a non-zero target, each projection adds the PI volume
+ * correction of macpressuresolver3.cpp:219-234 to every rhs row. */
+int shkz_b200_set_target_volume(shkz_b200_ctx *ctx, double current_volume, double target_volume);
+/* Volume-correction state {target_volume, current_volume, y_prev} as the
+ * reference serialises it (macpressuresolver3.cpp:320-342); post_initialize
+ * clears it. */
+int shkz_b200_get_volume_state(shkz_b200_ctx *ctx, double state[3]);
+int shkz_b200_set_volume_state(shkz_b200_ctx *ctx, const double state[3]);
+/* Warm-start vector (WarmStart=Yes): the previous solution indexed by the
+ * reference's unknown number, as m_prev_pressure holds it. size returns its
+ * length (0 before the first warm-started projection). */
+long long shkz_b200_warm_start_size(shkz_b200_ctx *ctx);
+int shkz_b200_get_warm_start(shkz_b200_ctx *ctx, double *out, size_t n);
+int shkz_b200_set_warm_start(shkz_b200_ctx *ctx, const double *in, size_t n);
 
 /* One pressure projection with host buffers: uploads, assembles, solves,
  * updates the velocities and downloads. Host arrays may be pageable; pinned

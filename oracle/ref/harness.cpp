@@ -10,6 +10,14 @@
 //
 // usage: shkz_ref_harness <in.bin> <out.bin> [Key=Value ...]
 //
+// Harness keys (the rest go to the reference's configuration):
+//   HarnessRepeat=N            project N times (velocity reset between them;
+//                              WarmStart=Yes carries the previous solution)
+//   HarnessSurfaceTension=k    surface_tension argument of project()
+//   HarnessDensity=<file>      set_solid_density() with face densities read
+//                              from <file> (double, x-fastest, dim 0..2)
+//   HarnessVolume=<cur>:<tgt>  set_target_volume(cur, tgt) before each call
+//
 // Input file (little endian):
 //   char[8] "SHKZIN01"; int32 nx,ny,nz, has_solid, has_solid_velocity;
 //   double dx, dt, fluid_band, solid_band;
@@ -52,6 +60,7 @@ public:
 	array3<Real> m_solid{this};
 	macarray3<Real> m_velocity{this};
 	macarray3<Real> m_solid_velocity{this};
+	macarray3<Real> m_density{this};
 	macproject3_driver m_macproject{this,"macpressuresolver3"};
 };
 }
@@ -158,6 +167,26 @@ int main( int argc, const char *argv[] ) {
 	}
 	std::fclose(fp);
 	//
+	const double kappa = dict.count("HarnessSurfaceTension") ? std::atof(dict["HarnessSurfaceTension"].c_str()) : 0.0;
+	if( dict.count("HarnessDensity") ) {
+		FILE *df = std::fopen(dict["HarnessDensity"].c_str(),"rb");
+		if( ! df ) { std::fprintf(stderr,"cannot open density file\n"); return 2; }
+		root.m_density.initialize(shape);
+		for( int dim=0; dim<3; ++dim ) {
+			const shape3 fs = shape.face(dim);
+			buf.resize(fs.count());
+			if( ! rd(df,buf.data(),buf.size())) { std::fprintf(stderr,"short density\n"); return 2; }
+			for( int k=0; k<fs.d; ++k ) for( int j=0; j<fs.h; ++j ) for( int i=0; i<fs.w; ++i ) {
+				root.m_density[dim].set(i,j,k,buf[i+(size_t)fs.w*(j+(size_t)fs.h*k)]);
+			}
+		}
+		std::fclose(df);
+		root.m_macproject->set_solid_density(&root.m_density);
+	}
+	double vol_cur (0.0), vol_tgt (0.0);
+	const bool has_volume = dict.count("HarnessVolume") > 0;
+	if( has_volume ) std::sscanf(dict["HarnessVolume"].c_str(),"%lf:%lf",&vol_cur,&vol_tgt);
+	//
 	FILE *out = std::fopen(argv[2],"wb");
 	if( ! out ) { std::fprintf(stderr,"cannot open %s\n",argv[2]); return 2; }
 	wr(out,"SHKZOUT1",8);
@@ -183,8 +212,9 @@ int main( int argc, const char *argv[] ) {
 	double best_ms = 1e300;
 	for( int rep=0; rep<std::max(1,repeat); ++rep ) {
 		if( rep ) set_velocity();
+		if( has_volume ) root.m_macproject->set_target_volume(vol_cur,vol_tgt);
 		auto t0 = std::chrono::steady_clock::now();
-		root.m_macproject->project(dt,velocity,solid,solid_velocity,fluid);
+		root.m_macproject->project(dt,velocity,solid,solid_velocity,fluid,kappa);
 		auto t1 = std::chrono::steady_clock::now();
 		best_ms = std::min(best_ms,std::chrono::duration<double,std::milli>(t1-t0).count());
 	}

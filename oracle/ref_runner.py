@@ -64,7 +64,7 @@ def read_system(path: str) -> dict:
 def run_reference(scene, variant: str = "float", mode: str = "mic0", tol: Optional[float] = None,
                   threads: Optional[int] = None, tile_size: int = 8, dump_system: bool = True,
                   repeat: int = 1, extra: Optional[dict] = None, linsolver: str = "refmic0",
-                  extra_libpath: Optional[list] = None) -> RefResult:
+                  extra_libpath: Optional[list] = None, density: Optional[list] = None) -> RefResult:
     exe = os.path.join(REF_DIR, variant, "shkz_ref_harness")
     if not os.path.exists(exe):
         raise FileNotFoundError(exe)
@@ -78,6 +78,12 @@ def run_reference(scene, variant: str = "float", mode: str = "mic0", tol: Option
                 f"Threads={threads or os.cpu_count()}", f"HarnessRepeat={repeat}"]
         for k, v in (extra or {}).items():
             args.append(f"{k}={v}")
+        if density is not None:
+            dpath = os.path.join(td, "density.bin")
+            with open(dpath, "wb") as f:
+                for d in range(3):
+                    f.write(np.ascontiguousarray(density[d], np.float64).tobytes())
+            args.append(f"HarnessDensity={dpath}")
         env = dict(os.environ)
         env["LD_LIBRARY_PATH"] = ":".join(list(extra_libpath or []) + [os.path.join(REF_DIR, variant),
                                                                           env.get("LD_LIBRARY_PATH", "")])

@@ -94,12 +94,29 @@ static int levelset_exist(const float *v, const unsigned char *active, size_t n)
     return 0;
 }
 
+/* one of the four nodes of face (d; i,j,k) is active in the solid grid */
+static int act_face(const unsigned char *solid_active, int nx, int ny, int d, int i, int j, int k)
+{
+    const int NX = nx + 1, NY = ny + 1;
+    /* the face spans the two axes other than d */
+    const int ax = d == 0 ? 1 : 0, ay = d == 2 ? 1 : 2;
+    int act = 0;
+    for (int b = 0; b < 2; ++b)
+        for (int a = 0; a < 2; ++a) {
+            int n[3] = {i, j, k};
+            n[ax] += a;
+            n[ay] += b;
+            act |= solid_active[IDX(n[0], n[1], n[2], NX, NY)];
+        }
+    return act;
+}
+
 void shkzo_fractions(int nx, int ny, int nz,
                      const float *solid, const unsigned char *solid_active,
                      const float *fluid, const unsigned char *fluid_active,
                      double eps_solid, double eps_fluid,
                      int second_order_fluid, int second_order_solid,
-                     float *area[3], float *rho[3])
+                     float *area[3], float *rho[3], float *const density[3])
 {
     const int NX = nx + 1, NY = ny + 1;
     const size_t nn = (size_t)(nx + 1) * (ny + 1) * (nz + 1);
@@ -155,6 +172,13 @@ void shkzo_fractions(int nx, int ny, int nz,
                         }
                     }
                     float af = (float)a;
+                    if (density && solid_exists && act_face(solid_active, nx, ny, d, i, j, k)) {
+                        /* set_solid_density: active faces of the area grid become
+                         * density*area + (1 - density) (macpressuresolver3.cpp:75-80) */
+                        const float dens = density[d][f];
+                        const float da = dens * af;
+                        af = (float)((double)da + (1.0 - (double)dens));
+                    }
                     if (!second_order_solid && af) af = 1.0f; /* macpressuresolver3.cpp:89-93 */
                     area[d][f] = af;
                     /* --- liquid fraction (macutility3.cpp:172-200) --- */
@@ -493,7 +517,7 @@ done:
 
 void shkzo_update_velocity(int nx, int ny, int nz, double dx, double dt, const float *pressure,
                            float *const area[3], float *const rho[3], float *const solid_velocity[3],
-                           float *velocity[3], unsigned char *velocity_active[3])
+                           float *velocity[3], unsigned char *velocity_active[3], float *const density[3])
 {
     /* macpressuresolver3.cpp:269-284; pressure is the float grid m_pressure
      * (0 = background where no unknown was written). */
@@ -516,6 +540,11 @@ void shkzo_update_velocity(int nx, int ny, int nz, double dx, double dt, const f
                             const float diff = +p1 - p0;
                             const float value = (float)(dt * diff / (r * dx));
                             velocity[d][f] = velocity[d][f] - value;
+                        }
+                        if (density) {
+                            /* macpressuresolver3.cpp:286-293 */
+                            const float scale = (float)(1.0 - (1.0 - (double)area[d][f]) * (double)density[d][f]);
+                            velocity[d][f] = scale * velocity[d][f];
                         }
                     } else {
                         velocity[d][f] = 0.0f; /* set_off: inactive, reads background 0 */

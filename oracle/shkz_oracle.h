@@ -12,7 +12,7 @@ void shkzo_fractions(int nx, int ny, int nz,
                      const float *fluid, const unsigned char *fluid_active,
                      double eps_solid, double eps_fluid,
                      int second_order_fluid, int second_order_solid,
-                     float *area[3], float *rho[3]);
+                     float *area[3], float *rho[3], float *const density[3]);
 long long shkzo_label(int nx, int ny, int nz, int tile, const float *fluid,
                       float *const area[3], float *const rho[3], long long *index);
 long long shkzo_assemble(int nx, int ny, int nz, double dx, double dt, const float *fluid,
@@ -29,7 +29,7 @@ int shkzo_pcg(long long n, const long long *indptr, const long long *indices, co
               double omega, double min_ratio, double *reresid_out);
 void shkzo_update_velocity(int nx, int ny, int nz, double dx, double dt, const float *pressure,
                            float *const area[3], float *const rho[3], float *const solid_velocity[3],
-                           float *velocity[3], unsigned char *velocity_active[3]);
+                           float *velocity[3], unsigned char *velocity_active[3], float *const density[3]);
 #ifdef __cplusplus
 }
 #endif

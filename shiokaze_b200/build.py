@@ -29,6 +29,7 @@ UNITS = {
     "learned.cu": [],
     "api.cu": [],
     "noalloc.cu": [],
+    "warmstart.cu": [],
 }
 HEADERS = ["common.cuh", "kernels.h", "solver.h", "learned.h", "tc_conv.cuh"]
 

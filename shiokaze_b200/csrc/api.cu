@@ -75,6 +75,19 @@ struct shkz_b200_ctx {
   int model_ready = 0;  // block activity computed for the current system
   AssemblyInputs last_in{};
   SolverState *st_scratch = nullptr;
+  // optional terms: surface tension curvature, volume correction, warm start
+  float *curv = nullptr;
+  size_t cap_curv = 0;
+  double vol_target = 0.0, vol_current = 0.0, vol_yprev = 0.0;
+  double *prev = nullptr;          // warm-start vector by reference unknown number
+  long long prev_n = 0, cap_prev = 0;
+  int *rank_pool = nullptr, *rank_cnt = nullptr;
+  long long *rank_total = nullptr;
+  double *xw = nullptr;            // warm-start x0 over the pool
+  int cap_warm_pool = 0;
+  size_t cap_rank_cnt = 0;
+  float *h_dens[3] = {};           // staging of the solid density faces (host path)
+  size_t cap_h_dens[3] = {0, 0, 0};
 };
 
 extern "C" void shkz_b200_default_config(shkz_b200_config *c) {
@@ -95,6 +108,9 @@ extern "C" void shkz_b200_default_config(shkz_b200_config *c) {
   c->stall_window = 8;
   c->device = 0;
   c->mic_block = 16;
+  c->gain = 1.0;
+  c->warm_start = 0;
+  c->index_tile = 16;
 }
 
 extern "C" const char *shkz_b200_errstr(int code) {
@@ -328,7 +344,9 @@ extern "C" void shkz_b200_destroy(shkz_b200_ctx *ctx) {
                   ctx->z64, ctx->x, ctx->r,
                   ctx->p, ctx->q, ctx->z, ctx->t, ctx->p32, ctx->partials, ctx->out4, ctx->counter, ctx->st,
                   ctx->wflags, ctx->faces_f, ctx->faces_b, ctx->ws, ctx->st_scratch, ctx->mcount, ctx->mstate,
-                  ctx->mtile, ctx->mnbr, ctx->msched, ctx->msub, ctx->mfaces_f, ctx->mfaces_b};
+                  ctx->mtile, ctx->mnbr, ctx->msched, ctx->msub, ctx->mfaces_f, ctx->mfaces_b, ctx->curv,
+                  ctx->prev, ctx->rank_pool, ctx->rank_cnt, ctx->rank_total, ctx->xw, ctx->h_dens[0],
+                  ctx->h_dens[1], ctx->h_dens[2]};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (ctx->model) learned_free(ctx->model);
@@ -502,7 +520,9 @@ static int solve_system(shkz_b200_ctx *ctx, double tol, int precond, shkz_b200_r
 // preconditioner is the FP32 MIC(0) applied to the scaled residual. It
 // solves the same FP64 system the reference assembles, to fp64_tol, into
 // xref64, and reports ||x64 - xref64||inf / ||xref64||inf.
-static int fp64_reference_solve(shkz_b200_ctx *ctx, shkz_b200_result *res) {
+// x0 (may be null): warm-start vector already added to x64; the reference
+// solution of the shifted system gets it too before the comparison.
+static int fp64_reference_solve(shkz_b200_ctx *ctx, shkz_b200_result *res, const double *x0) {
   cudaStream_t s = ctx->stream;
   const PoolSystem S = pool_system(ctx);
   const int n = ctx->K * SHKZ_TC;
@@ -557,6 +577,7 @@ static int fp64_reference_solve(shkz_b200_ctx *ctx, shkz_b200_result *res) {
   SHKZ_CUDA_TRY(cudaMemcpyAsync(h, ctx->out4, sizeof(double) * 4, cudaMemcpyDeviceToHost, s));
   SHKZ_CUDA_TRY(cudaStreamSynchronize(s));
   res->fp64_reresid = h[0] / h[2];
+  if (x0) launch_axpy2_64(n, 1.0, x0, ctx->xref64, x0, ctx->p64, s);  // xref64 += x0 (p64 scratch)
   // error: ||x64 - xref64||inf over ||xref64||inf  (q64 = x64 - xref64)
   SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->q64, ctx->x64, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
   launch_axpy2_64(n, -1.0, ctx->xref64, ctx->q64, ctx->xref64, ctx->p64, s);  // second pair is a scratch write
@@ -577,6 +598,8 @@ static int validate(const shkz_b200_project_args *a) {
   for (int d = 0; d < 3; ++d)
     if (!a->velocity[d] || !a->velocity_active[d]) return SHKZ_B200_ERR_ARG;
   if (!(a->dx > 0.0)) return SHKZ_B200_ERR_ARG;
+  const bool dens = a->solid_density[0] || a->solid_density[1] || a->solid_density[2];
+  if (dens && !(a->solid_density[0] && a->solid_density[1] && a->solid_density[2])) return SHKZ_B200_ERR_ARG;
   return 0;
 }
 
@@ -584,6 +607,39 @@ static float ms_between(cudaEvent_t a, cudaEvent_t b) {
   float ms = 0.f;
   cudaEventElapsedTime(&ms, a, b);
   return ms;
+}
+
+// warm-start buffers: pool-sized rank and x0, reference-tile counts, and the
+// previous vector (kept across growth)
+static int ensure_warm(shkz_b200_ctx *ctx, const Geometry &G, int T, long long unknowns_bound) {
+  if (ctx->cap_warm_pool < ctx->cap_pool) {
+    GROW(rank_pool, (size_t)ctx->cap_pool * SHKZ_TC);
+    GROW(xw, (size_t)ctx->cap_pool * SHKZ_TC);
+    ctx->cap_warm_pool = ctx->cap_pool;
+  }
+  const size_t nref = unknown_rank_scratch(G, T);
+  if (nref > ctx->cap_rank_cnt) {
+    GROW(rank_cnt, nref);
+    ctx->cap_rank_cnt = nref;
+  }
+  if (!ctx->rank_total) GROW(rank_total, 1);
+  if (unknowns_bound > ctx->cap_prev) {
+    const long long cap = unknowns_bound + unknowns_bound / 4 + 1024;
+    double *np = nullptr;
+    cudaError_t e = cudaMalloc(&np, sizeof(double) * (size_t)cap);
+    if (e != cudaSuccess) {
+      shkz_set_cuda_error(e, "cudaMalloc", __FILE__, __LINE__);
+      return SHKZ_B200_ERR_NOMEM;
+    }
+    if (ctx->prev && ctx->prev_n > 0)
+      SHKZ_CUDA_TRY(cudaMemcpyAsync(np, ctx->prev, sizeof(double) * (size_t)ctx->prev_n, cudaMemcpyDeviceToDevice,
+                                    ctx->stream));
+    SHKZ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    if (ctx->prev) cudaFree(ctx->prev);
+    ctx->prev = np;
+    ctx->cap_prev = cap;
+  }
+  return 0;
 }
 
 static int project_device(shkz_b200_ctx *ctx, const shkz_b200_project_args *a, shkz_b200_result *res) {
@@ -607,11 +663,24 @@ static int project_device(shkz_b200_ctx *ctx, const shkz_b200_project_args *a, s
   in.eps_fluid = ctx->cfg.eps_fluid;
   in.second_order_fluid = ctx->cfg.second_order_fluid;
   in.second_order_solid = ctx->cfg.second_order_solid;
+  for (int d = 0; d < 3; ++d) in.density[d] = a->solid_density[d];
+  in.rhs_add = 0.0;
 
   ctx->last_in = in;
   const long long launches0 = launches_so_far();
   cudaEventRecord(ctx->ev[0], s);
   launch_label(in, ctx->flags, ctx->unk, ctx->tile_count, s);
+  if (a->surface_tension != 0.0) {
+    // velocity += surface tension force before the system is built (it reads the new velocity)
+    const size_t cells = (size_t)G.nx * G.ny * G.nz;
+    if (cells > ctx->cap_curv) {
+      GROW(curv, cells);
+      ctx->cap_curv = cells;
+    }
+    float *vel[3] = {a->velocity[0], a->velocity[1], a->velocity[2]};
+    const uint8_t *vact[3] = {a->velocity_active[0], a->velocity_active[1], a->velocity_active[2]};
+    launch_surface_tension(in, ctx->flags, ctx->curv, a->surface_tension, vel, vact, s);
+  }
   // pool size (one small host read), then the pool itself
   const int K = pool_count(G, ctx->tile_count, ctx->bsum, ctx->total, s);
   if (K < 0) {
@@ -629,9 +698,34 @@ static int project_device(shkz_b200_ctx *ctx, const shkz_b200_project_args *a, s
   ctx->G = G;
   ctx->model_ready = 0;
   res->tiles = K;
+  res->volume_rhs_correct = 0.0;
+  if (K > 0 && ctx->cfg.gain != 0.0 && ctx->vol_target != 0.0) {
+    // PI volume correction (macpressuresolver3.cpp:219-234), state advanced once per solved projection
+    const double x = (ctx->vol_current - ctx->vol_target) / ctx->vol_target;
+    const double y = ctx->vol_yprev + x * a->dt;
+    ctx->vol_yprev = y;
+    const double kp = ctx->cfg.gain * 2.3 / (25.0 * 0.01);
+    const double ki = kp * kp / 16.0;
+    in.rhs_add = -(kp * x + ki * y) / (x + 1.0);
+    res->volume_rhs_correct = in.rhs_add;
+    ctx->last_in = in;
+  }
   CoeffOutputs co{ctx->diag, ctx->offx, ctx->offy, ctx->offz, ctx->diag64, ctx->offx64, ctx->offy64, ctx->offz64,
                   ctx->rhs64};
   launch_coeff(in, ctx->flags, ctx->pool_tile, K, ctx->unk, co, s);
+  const bool warm = K > 0 && ctx->cfg.warm_start;
+  if (warm) {
+    // b <- b - A x_prev with x_prev read by the reference's unknown number
+    const int T = ctx->cfg.index_tile > 0 ? ctx->cfg.index_tile : 16;
+    rc = ensure_warm(ctx, G, T, (long long)K * SHKZ_TC);
+    if (rc) return rc;
+    const PoolSystem S0 = pool_system(ctx);
+    launch_unknown_rank(G, K, ctx->unk, T, ctx->tile_state, ctx->rank_pool, ctx->rank_cnt, ctx->rank_total, s);
+    launch_warm_gather((long long)K * SHKZ_TC, ctx->rank_pool, ctx->prev, ctx->prev_n, ctx->xw, s);
+    launch_residual64(S0, ctx->rhs64, ctx->xw, ctx->r64, ctx->partials, ctx->counter + 2, ctx->out4, s);
+    SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->rhs64, ctx->r64, sizeof(double) * (size_t)K * SHKZ_TC,
+                                  cudaMemcpyDeviceToDevice, s));
+  }
   const int precond = ctx->cfg.preconditioner;
   const PoolSystem S = pool_system(ctx);
   ctx->mic_ready = 0;
@@ -666,6 +760,11 @@ static int project_device(shkz_b200_ctx *ctx, const shkz_b200_project_args *a, s
   cudaEventRecord(ctx->ev[2], s);
   // FP32 pressure of the solution, then the velocity update
   const int n = K * SHKZ_TC;
+  if (warm) {
+    // x = d + x_prev, and the new previous vector (length = unknown count)
+    launch_warm_finish(n, ctx->rank_pool, ctx->xw, ctx->x64, ctx->prev, s);
+    ctx->prev_n = ctx->unknowns;
+  }
   if (K > 0) launch_to_float(n, ctx->x64, ctx->p32, s);
   float *vel[3] = {a->velocity[0], a->velocity[1], a->velocity[2]};
   uint8_t *vact[3] = {a->velocity_active[0], a->velocity_active[1], a->velocity_active[2]};
@@ -678,7 +777,7 @@ static int project_device(shkz_b200_ctx *ctx, const shkz_b200_project_args *a, s
   res->err_fp64_inf = -1.0;
   res->fp64_reresid = -1.0;
   if (K > 0 && ctx->cfg.fp64_reference) {
-    int rrc = fp64_reference_solve(ctx, res);
+    int rrc = fp64_reference_solve(ctx, res, warm ? ctx->xw : nullptr);
     if (rrc && !solve_rc) solve_rc = rrc;
   }
   SHKZ_CUDA_TRY(cudaStreamSynchronize(s));
@@ -733,6 +832,13 @@ extern "C" int shkz_b200_project_host(shkz_b200_ctx *ctx, const shkz_b200_projec
     SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->h_vact[d], a->velocity_active[d], nf[d], cudaMemcpyHostToDevice, s));
     if (svel[d])
       SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->h_svel[d], a->solid_velocity[d], nf[d] * 4, cudaMemcpyHostToDevice, s));
+    if (a->solid_density[d]) {
+      if (nf[d] > ctx->cap_h_dens[d]) {
+        GROW(h_dens[d], nf[d]);
+        ctx->cap_h_dens[d] = nf[d];
+      }
+      SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->h_dens[d], a->solid_density[d], nf[d] * 4, cudaMemcpyHostToDevice, s));
+    }
   }
   cudaEventRecord(e1, s);
   shkz_b200_project_args da = *a;
@@ -744,6 +850,7 @@ extern "C" int shkz_b200_project_host(shkz_b200_ctx *ctx, const shkz_b200_projec
     da.velocity[d] = ctx->h_vel[d];
     da.velocity_active[d] = ctx->h_vact[d];
     da.solid_velocity[d] = svel[d] ? ctx->h_svel[d] : nullptr;
+    da.solid_density[d] = a->solid_density[d] ? ctx->h_dens[d] : nullptr;
   }
   da.pressure = ctx->h_pressure;
   da.pressure_active = ctx->h_pact;
@@ -1184,6 +1291,62 @@ static int learned_solve(shkz_b200_ctx *ctx, double tol, shkz_b200_result *res) 
   res->reresid = rmax_true / bmax;
   res->reresid_l2 = std::sqrt(r2 / b2);
   return rc;
+}
+
+extern "C" int shkz_b200_set_target_volume(shkz_b200_ctx *ctx, double current_volume, double target_volume) {
+  if (!ctx) return SHKZ_B200_ERR_ARG;
+  ctx->vol_current = current_volume;
+  ctx->vol_target = target_volume;
+  return 0;
+}
+
+extern "C" int shkz_b200_get_volume_state(shkz_b200_ctx *ctx, double state[3]) {
+  if (!ctx || !state) return SHKZ_B200_ERR_ARG;
+  state[0] = ctx->vol_target;
+  state[1] = ctx->vol_current;
+  state[2] = ctx->vol_yprev;
+  return 0;
+}
+
+extern "C" int shkz_b200_set_volume_state(shkz_b200_ctx *ctx, const double state[3]) {
+  if (!ctx || !state) return SHKZ_B200_ERR_ARG;
+  ctx->vol_target = state[0];
+  ctx->vol_current = state[1];
+  ctx->vol_yprev = state[2];
+  return 0;
+}
+
+extern "C" long long shkz_b200_warm_start_size(shkz_b200_ctx *ctx) { return ctx ? ctx->prev_n : -1; }
+
+extern "C" int shkz_b200_get_warm_start(shkz_b200_ctx *ctx, double *out, size_t n) {
+  if (!ctx || (n && !out) || (long long)n != ctx->prev_n) return SHKZ_B200_ERR_ARG;
+  if (n == 0) return 0;
+  cudaSetDevice(ctx->device);
+  SHKZ_CUDA_TRY(cudaMemcpyAsync(out, ctx->prev, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  SHKZ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+extern "C" int shkz_b200_set_warm_start(shkz_b200_ctx *ctx, const double *in, size_t n) {
+  if (!ctx || (n && !in)) return SHKZ_B200_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  if ((long long)n > ctx->cap_prev) {
+    const long long cap = (long long)n + 1024;
+    double *np = nullptr;
+    cudaError_t e = cudaMalloc(&np, sizeof(double) * (size_t)cap);
+    if (e != cudaSuccess) {
+      shkz_set_cuda_error(e, "cudaMalloc", __FILE__, __LINE__);
+      return SHKZ_B200_ERR_NOMEM;
+    }
+    SHKZ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    if (ctx->prev) cudaFree(ctx->prev);
+    ctx->prev = np;
+    ctx->cap_prev = cap;
+  }
+  if (n) SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->prev, in, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+  SHKZ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  ctx->prev_n = (long long)n;
+  return 0;
 }
 
 extern "C" int shkz_b200_learned_init(shkz_b200_ctx *ctx, unsigned seed) {

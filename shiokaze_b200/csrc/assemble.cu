@@ -12,6 +12,9 @@
 //   unknowns          mark_body (src/projection/macpressuresolver3.cpp:134-158)
 //   weights, rhs      macpressuresolver3.cpp:179-216
 //   velocity update   macpressuresolver3.cpp:262-284
+//   solid density     macpressuresolver3.cpp:75-80 (areas), 286-293 (velocity scale)
+//   surface tension   macpressuresolver3.cpp:98-128
+//   volume correction macpressuresolver3.cpp:219-234 (constant added to every rhs row)
 #include "common.cuh"
 #include "kernels.h"
 #include <float.h>
@@ -26,6 +29,7 @@ struct FaceParams {
   int solid_exists, fluid_exists;
   double eps_solid, eps_fluid;
   int second_order_fluid, second_order_solid;
+  const float *density[3];     // per-face solid density (set_solid_density), or null
 };
 
 // Marching-squares area of the negative region on the unit square, corners
@@ -83,6 +87,7 @@ __device__ float face_area(const FaceParams &P, int d, int i, int j, int k) {
   const int pd = d == 0 ? i : (d == 1 ? j : k);
   const int nd = d == 0 ? P.nx : (d == 1 ? P.ny : P.nz);
   double a;
+  bool act = false;  // face active in the reference's area grid
   if (!P.solid_exists) {
     // areas.clear(1.0) with the domain walls closed (macutility3.cpp:158-170)
     a = (pd == 0 || pd == nd) ? 0.0 : 1.0;
@@ -105,7 +110,7 @@ __device__ float face_area(const FaceParams &P, int d, int i, int j, int k) {
     const size_t s2 = nidx(P, n2[0], n2[1], n2[2]), s3 = nidx(P, n3[0], n3[1], n3[2]);
     // quadsolid[0][0], [1][0], [1][1], [0][1] -> corners (0,0),(1,0),(1,1),(0,1)
     const double v[4] = {(double)P.solid[s0], (double)P.solid[s1], (double)P.solid[s2], (double)P.solid[s3]};
-    const bool act = P.solid_active[s0] | P.solid_active[s1] | P.solid_active[s2] | P.solid_active[s3];
+    act = P.solid_active[s0] | P.solid_active[s1] | P.solid_active[s2] | P.solid_active[s3];
     if (act) {
       if (pd == 0 || pd == nd) a = 0.0;
       else a = 1.0 - get_area4(v);
@@ -117,6 +122,13 @@ __device__ float face_area(const FaceParams &P, int d, int i, int j, int k) {
     }
   }
   float af = (float)a;
+  if (act && P.density[d]) {
+    // solid density on the active faces of the area grid: density*area + (1 - density)
+    const int fw = P.nx + (d == 0), fh = P.ny + (d == 1);
+    const float dens = P.density[d][(size_t)i + (size_t)fw * ((size_t)j + (size_t)fh * (size_t)k)];
+    const float da = dens * af;
+    af = (float)((double)da + (1.0 - (double)dens));
+  }
   if (!P.second_order_solid && af != 0.0f) af = 1.0f;
   return af;
 }
@@ -209,7 +221,7 @@ __global__ void __launch_bounds__(256) k_coeff(FaceParams P, Geometry G, const i
                                                const float *vel2, const float *svel0, const float *svel1,
                                                const float *svel2, double dx, double dt, float *diag, float *offx,
                                                float *offy, float *offz, double *diag64, double *offx64,
-                                               double *offy64, double *offz64, double *rhs64) {
+                                               double *offy64, double *offz64, double *rhs64, double rhs_add) {
   P.fluid_exists = (*flags) & 1;
   P.solid_exists = P.solid ? (((*flags) >> 1) & 1) : 0;
   const int pt = blockIdx.x;
@@ -246,6 +258,7 @@ __global__ void __launch_bounds__(256) k_coeff(FaceParams P, Geometry G, const i
           b += -s * (1.0 - area) * us / dx;
         }
       }
+      b += rhs_add;
     }
     diag[o] = (float)dg;
     offx[o] = (float)lo[0];
@@ -297,9 +310,58 @@ __global__ void k_velocity_update(FaceParams P, Geometry G, const int *flags, in
         const float value = (float)(dt * (double)diff / ((double)rhof * dx));
         vel[f] = vel[f] - value;
       }
+      if (P.density[d]) {
+        const float scale = (float)(1.0 - (1.0 - (double)area) * (double)P.density[d][f]);
+        vel[f] = scale * vel[f];
+      }
     } else {
       vel[f] = 0.0f;
       vact[f] = 0;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Surface tension (macpressuresolver3.cpp:98-128): curvature as the 7-point
+// Laplacian of the liquid level set with clamped neighbours, then every active
+// face with 0 < rho < 1 gets u += -sgn*dt/(dx*rho)*kappa*kappa_face, the face
+// curvature interpolated by the liquid fraction.
+__global__ void k_curvature(FaceParams P, double dx, float *curv) {
+  const size_t n = (size_t)P.nx * P.ny * P.nz;
+  for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(c % P.nx), j = (int)((c / P.nx) % P.ny), k = (int)(c / ((size_t)P.nx * P.ny));
+    auto f = [&](int a, int b, int e) -> float {
+      a = min(max(a, 0), P.nx - 1);
+      b = min(max(b, 0), P.ny - 1);
+      e = min(max(e, 0), P.nz - 1);
+      return P.fluid[cidx(P, a, b, e)];
+    };
+    // the six neighbours are summed in FP32, as the reference's float operands are
+    const float s6 = f(i - 1, j, k) + f(i + 1, j, k) + f(i, j - 1, k) + f(i, j + 1, k) + f(i, j, k - 1) + f(i, j, k + 1);
+    const double value = ((double)s6 - 6.0 * (double)P.fluid[c]) / (dx * dx);
+    curv[c] = (float)value;
+  }
+}
+
+__global__ void k_surface_tension(FaceParams P, Geometry G, const int *flags, int d, const float *curv, double kappa,
+                                  double dx, double dt, float *vel, const uint8_t *vact) {
+  P.fluid_exists = (*flags) & 1;
+  P.solid_exists = P.solid ? (((*flags) >> 1) & 1) : 0;
+  const int fw = G.nx + (d == 0), fh = G.ny + (d == 1), fd = G.nz + (d == 2);
+  const size_t nf = (size_t)fw * fh * fd;
+  for (size_t f = blockIdx.x * (size_t)blockDim.x + threadIdx.x; f < nf; f += (size_t)gridDim.x * blockDim.x) {
+    if (!vact[f]) continue;
+    const int i = (int)(f % fw), j = (int)((f / fw) % fh), k = (int)(f / ((size_t)fw * fh));
+    const double rho = (double)face_rho(P, d, i, j, k);
+    if (rho != 0.0 && rho < 1.0) {
+      const int ci = min(i, G.nx - 1), cj = min(j, G.ny - 1), ck = min(k, G.nz - 1);
+      const int bi = max(i - (d == 0), 0), bj = max(j - (d == 1), 0), bk = max(k - (d == 2), 0);
+      const size_t c1 = cidx(P, ci, cj, ck), c0 = cidx(P, min(bi, G.nx - 1), min(bj, G.ny - 1), min(bk, G.nz - 1));
+      const double sgn = P.fluid[c1] < 0.0f ? -1.0 : 1.0;
+      const double theta = sgn < 0 ? 1.0 - rho : rho;
+      const double face_c = theta * (double)curv[c1] + (1.0 - theta) * (double)curv[c0];
+      const float inc = (float)(-sgn * dt / (dx * rho) * kappa * face_c);
+      vel[f] = vel[f] + inc;
     }
   }
 }
@@ -336,6 +398,7 @@ static FaceParams make_params(const AssemblyInputs &in) {
   P.eps_fluid = in.eps_fluid;
   P.second_order_fluid = in.second_order_fluid;
   P.second_order_solid = in.second_order_solid;
+  for (int d = 0; d < 3; ++d) P.density[d] = in.density[d];
   return P;
 }
 
@@ -355,7 +418,18 @@ void launch_coeff(const AssemblyInputs &in, const int *flags, const int *pool_ti
   count_launches(1);
   k_coeff<<<K, 256, 0, s>>>(make_params(in), in.G, flags, pool_tile, unk, in.vel[0], in.vel[1], in.vel[2],
                              in.svel[0], in.svel[1], in.svel[2], in.dx, in.dt, out.diag, out.offx, out.offy, out.offz,
-                             out.diag64, out.offx64, out.offy64, out.offz64, out.rhs64);
+                             out.diag64, out.offx64, out.offy64, out.offz64, out.rhs64, in.rhs_add);
+}
+
+void launch_surface_tension(const AssemblyInputs &in, const int *flags, float *curv, double kappa, float *const vel[3],
+                            const uint8_t *const vact[3], cudaStream_t s) {
+  count_launches(1);
+  k_curvature<<<148 * 16, 256, 0, s>>>(make_params(in), in.dx, curv);
+  for (int d = 0; d < 3; ++d) {
+    count_launches(1);
+    k_surface_tension<<<148 * 16, 256, 0, s>>>(make_params(in), in.G, flags, d, curv, kappa, in.dx, in.dt, vel[d],
+                                               vact[d]);
+  }
 }
 
 void launch_velocity_update(const AssemblyInputs &in, const int *flags, const int *tile_state,

@@ -15,6 +15,8 @@ struct AssemblyInputs {
   double dx, dt;
   double eps_solid, eps_fluid;
   int second_order_fluid, second_order_solid;
+  const float *density[3];     // per-face solid density, each may be null
+  double rhs_add;              // volume correction added to every rhs row
 };
 
 struct CoeffOutputs {
@@ -44,7 +46,18 @@ void launch_coeff(const AssemblyInputs &in, const int *flags, const int *pool_ti
                   const CoeffOutputs &out, cudaStream_t s);
 void launch_velocity_update(const AssemblyInputs &in, const int *flags, const int *tile_state,
                             const float *pressure_pool, float *const vel[3], uint8_t *const vact[3], cudaStream_t s);
+void launch_surface_tension(const AssemblyInputs &in, const int *flags, float *curv, double kappa, float *const vel[3],
+                            const uint8_t *const vact[3], cudaStream_t s);
 void launch_scatter_pressure(const Geometry &G, const int *tile_state, const float *pressure_pool, const uint8_t *unk,
                              float *pressure, uint8_t *pressure_active, cudaStream_t s);
+
+// warmstart.cu: reference unknown numbering (tiles of edge T, x fastest) and
+// the warm-start gather/finish over the pool
+size_t unknown_rank_scratch(const Geometry &G, int T);
+long long launch_unknown_rank(const Geometry &G, int K, const uint8_t *unk, int T, const int *tile_state,
+                              int *rank_pool, int *cnt, long long *d_total, cudaStream_t s);
+void launch_warm_gather(long long n, const int *rank_pool, const double *prev, long long prev_n, double *x0,
+                        cudaStream_t s);
+void launch_warm_finish(long long n, const int *rank_pool, const double *x0, double *x, double *prev, cudaStream_t s);
 
 }  // namespace shkz

@@ -41,7 +41,10 @@ class Config(ctypes.Structure):
         ("stall_window", ctypes.c_int),
         ("device", ctypes.c_int),
         ("mic_block", ctypes.c_int),
-        ("reserved", ctypes.c_int * 7),
+        ("gain", ctypes.c_double),
+        ("warm_start", ctypes.c_int),
+        ("index_tile", ctypes.c_int),
+        ("reserved", ctypes.c_int * 4),
     ]
 
 
@@ -54,6 +57,8 @@ class ProjectArgs(ctypes.Structure):
         ("velocity", ctypes.c_void_p * 3), ("velocity_active", ctypes.c_void_p * 3),
         ("solid_velocity", ctypes.c_void_p * 3),
         ("pressure", ctypes.c_void_p), ("pressure_active", ctypes.c_void_p),
+        ("surface_tension", ctypes.c_double),
+        ("solid_density", ctypes.c_void_p * 3),
     ]
 
 
@@ -64,7 +69,8 @@ class Result(ctypes.Structure):
         ("reresid", ctypes.c_double), ("reresid_l2", ctypes.c_double), ("err_fp64_inf", ctypes.c_double),
         ("fp64_reresid", ctypes.c_double), ("ms_assemble", ctypes.c_double), ("ms_solve", ctypes.c_double),
         ("ms_update", ctypes.c_double), ("ms_total", ctypes.c_double), ("ms_h2d", ctypes.c_double),
-        ("ms_d2h", ctypes.c_double), ("kernel_launches", ctypes.c_longlong), ("reserved", ctypes.c_double * 7),
+        ("ms_d2h", ctypes.c_double), ("kernel_launches", ctypes.c_longlong),
+        ("volume_rhs_correct", ctypes.c_double), ("reserved", ctypes.c_double * 6),
     ]
 
     def as_dict(self):
@@ -80,6 +86,8 @@ EXPORTS = [
     "shkz_b200_learned_get_params", "shkz_b200_learned_apply", "shkz_b200_learned_dims",
     "shkz_b200_learned_tensor", "shkz_b200_learned_backward", "shkz_b200_learned_train",
     "shkz_b200_learned_save", "shkz_b200_learned_load", "shkz_b200_conv3d", "shkz_b200_conv3d_noalloc",
+    "shkz_b200_set_target_volume", "shkz_b200_get_volume_state", "shkz_b200_set_volume_state",
+    "shkz_b200_warm_start_size", "shkz_b200_get_warm_start", "shkz_b200_set_warm_start",
 ]
 
 _lib = None
@@ -109,6 +117,13 @@ def load(path: str = LIB_PATH):
     L.shkz_b200_stream.restype = P
     L.shkz_b200_solve_csr.argtypes = [P, ctypes.c_longlong, P, P, P, P, P, ctypes.POINTER(Result)]
     L.shkz_b200_inspect.argtypes = [P, ctypes.c_int, P, ctypes.c_size_t]
+    L.shkz_b200_set_target_volume.argtypes = [P, ctypes.c_double, ctypes.c_double]
+    L.shkz_b200_get_volume_state.argtypes = [P, P]
+    L.shkz_b200_set_volume_state.argtypes = [P, P]
+    L.shkz_b200_warm_start_size.argtypes = [P]
+    L.shkz_b200_warm_start_size.restype = ctypes.c_longlong
+    L.shkz_b200_get_warm_start.argtypes = [P, P, ctypes.c_size_t]
+    L.shkz_b200_set_warm_start.argtypes = [P, P, ctypes.c_size_t]
     L.shkz_b200_apply_preconditioner.argtypes = [P, P, P]
     L.shkz_b200_apply_matrix.argtypes = [P, P, P]
     L.shkz_b200_time_kernel.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),

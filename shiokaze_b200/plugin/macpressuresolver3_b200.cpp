@@ -14,7 +14,12 @@
  *     the reference switches off, and keeps the pressure in an array3 that
  *     get_pressure() returns;
  *   - records the same timer labels and the iteration count under
- *     <ArgName>_number_projection_iteration (macpressuresolver3.cpp:253).
+ *     <ArgName>_number_projection_iteration (macpressuresolver3.cpp:253);
+ *   - honours the optional terms: surface_tension, set_solid_density,
+ *     set_target_volume with Gain (recording <ArgName>_volume_correct_rhs),
+ *     and WarmStart, whose previous-solution vector is numbered by the
+ *     grids' TileSize exactly as the reference numbers its unknowns and is
+ *     serialised through the RCMatrix module's own vector format.
  * The host side only packs the array3/macarray3 grids into dense buffers and
  * calls the C ABI (include/shkz_b200.h); all arithmetic runs on the GPU.
  * Errors never throw: a failed solve is reported on the console and the
@@ -23,9 +28,11 @@
 #include <shiokaze/array/array3.h>
 #include <shiokaze/array/macarray3.h>
 #include <shiokaze/projection/macproject3_interface.h>
+#include <shiokaze/math/RCMatrix_interface.h>
 #include <shiokaze/core/console.h>
 #include <shiokaze/core/timer.h>
 #include "shkz_b200.h"
+#include <algorithm>
 #include <cstring>
 #include <vector>
 //
@@ -70,9 +77,6 @@ protected:
 		//
 		scoped_timer timer(this);
 		timer.tick(); console::dump( ">>> Pressure Projection (B200) started...\n" );
-		if( surface_tension || m_solid_density || (m_param.gain && m_target_volume) ) {
-			console::dump( "Surface tension, solid density and volume correction are not supported by the B200 projection; ignored.\n" );
-		}
 		if( ! m_ctx ) {
 			int rc = shkz_b200_create(&m_ctx,&m_cfg);
 			if( rc ) {
@@ -80,9 +84,15 @@ protected:
 				console::write(get_argument_name()+"_number_projection_iteration", 0);
 				return;
 			}
+			if( m_prev_pending ) {
+				shkz_b200_set_warm_start(m_ctx,m_prev_host.data(),m_prev_host.size());
+				m_prev_pending = false;
+			}
 		} else {
 			shkz_b200_set_config(m_ctx,&m_cfg);
 		}
+		const double vstate[3] = { m_target_volume, m_current_volume, m_y_prev };
+		shkz_b200_set_volume_state(m_ctx,vstate);
 		//
 		timer.tick(); console::dump( "Packing grids..." );
 		pack(fluid,m_fluid,m_fluid_active);
@@ -91,6 +101,7 @@ protected:
 		for( int dim=0; dim<3; ++dim ) {
 			pack(velocity[dim],m_vel[dim],m_vact[dim]);
 			pack(solid_velocity[dim],m_svel[dim],m_svact[dim]);
+			if( m_solid_density ) pack((*m_solid_density)[dim],m_dens[dim],m_dact[dim]);
 		}
 		console::dump( "Done. Took %s\n", timer.stock("pack_grids").c_str());
 		//
@@ -109,10 +120,17 @@ protected:
 		m_pact.resize(m_shape.count());
 		a.pressure = m_p.data();
 		a.pressure_active = m_pact.data();
+		a.surface_tension = surface_tension;
+		if( m_solid_density ) for( int dim=0; dim<3; ++dim ) a.solid_density[dim] = m_dens[dim].data();
 		//
 		timer.tick(); console::dump( "Projecting on the GPU...");
 		shkz_b200_result res;
 		const int rc = shkz_b200_project_host(m_ctx,&a,&res);
+		double vnew[3];
+		if( shkz_b200_get_volume_state(m_ctx,vnew) == 0 ) m_y_prev = vnew[2];
+		if( res.unknowns && m_param.gain && m_target_volume ) {
+			console::write(get_argument_name()+"_volume_correct_rhs", res.volume_rhs_correct);
+		}
 		console::write(get_argument_name()+"_number_projection_iteration", rc ? 0 : res.iterations);
 		console::write(get_argument_name()+"_reresid_inf", res.reresid);
 		console::write(get_argument_name()+"_reresid_l2", res.reresid_l2);
@@ -151,6 +169,12 @@ protected:
 		config.get_bool("SecondOrderAccurateFluid",m_param.second_order_accurate_fluid,"Whether to enforce second order accuracy");
 		config.get_bool("SecondOrderAccurateSolid",m_param.second_order_accurate_solid,"Whether to enforce second order accuracy for solid surfaces");
 		config.get_double("Gain",m_param.gain,"Rate for volume correction");
+		config.get_bool("WarmStart",m_param.warm_start,"Start from the solution of previous pressure");
+		unsigned tile = m_cfg.index_tile;
+		config.get_unsigned("TileSize",tile,"Tile size per dimension");
+		m_cfg.index_tile = tile;
+		m_cfg.gain = m_param.gain;
+		m_cfg.warm_start = m_param.warm_start;
 		config.get_double("Residual",m_cfg.residual,"Tolerable residual");
 		unsigned max_it = m_cfg.max_iterations;
 		config.get_unsigned("MaxIterations",max_it,"Maximal iteration count");
@@ -179,14 +203,23 @@ protected:
 		m_pressure.initialize(m_shape);
 		m_target_volume = m_current_volume = m_y_prev = 0.0;
 	}
-	// Same fields in the same order as macpressuresolver3 (:320-342), so
-	// saved states load in either module (warm start is not supported here).
+	// Same fields in the same order as macpressuresolver3 (:320-342), the
+	// warm-start vector through the RCMatrix module's own vector format, so
+	// saved states load in either module.
 	virtual void initialize( const filestream &file ) override {
 		file.r(m_shape);
 		file.r(m_dx);
 		file.r(m_target_volume);
 		file.r(m_current_volume);
 		file.r(m_y_prev);
+		if( m_param.warm_start ) {
+			auto v = m_factory->allocate_vector();
+			v->initialize(file);
+			m_prev_host.resize(v->size());
+			for( size_t n=0; n<m_prev_host.size(); ++n ) m_prev_host[n] = v->at(n);
+			if( m_ctx ) shkz_b200_set_warm_start(m_ctx,m_prev_host.data(),m_prev_host.size());
+			else m_prev_pending = true;
+		}
 	}
 	virtual void serialize( const filestream &file ) const override {
 		file.w(m_shape);
@@ -194,6 +227,18 @@ protected:
 		file.w(m_target_volume);
 		file.w(m_current_volume);
 		file.w(m_y_prev);
+		if( m_param.warm_start ) {
+			std::vector<double> prev;
+			if( m_ctx ) {
+				prev.resize((size_t)std::max(0LL,shkz_b200_warm_start_size(m_ctx)));
+				shkz_b200_get_warm_start(m_ctx,prev.data(),prev.size());
+			} else {
+				prev = m_prev_host;
+			}
+			auto v = m_factory->allocate_vector(prev.size());
+			for( size_t n=0; n<prev.size(); ++n ) v->set(n,prev[n]);
+			v->serialize(file);
+		}
 	}
 	virtual const array3<Real> * get_pressure() const override {
 		return &m_pressure;
@@ -203,6 +248,7 @@ protected:
 		double gain {1.0};
 		bool second_order_accurate_fluid {true};
 		bool second_order_accurate_solid {true};
+		bool warm_start {false};
 	};
 	Parameters m_param;
 	shkz_b200_config m_cfg = make_default_config();
@@ -220,9 +266,12 @@ protected:
 	double m_current_volume {0.0};
 	double m_y_prev {0.0};
 	const macarray3<Real> *m_solid_density {nullptr};
+	RCMatrix_factory_driver<size_t,double> m_factory{this,"RCMatrix"};
+	std::vector<double> m_prev_host;
+	bool m_prev_pending {false};
 	// host staging
-	std::vector<float> m_fluid, m_solid, m_vel[3], m_svel[3], m_p;
-	std::vector<uint8_t> m_fluid_active, m_solid_active, m_vact[3], m_svact[3], m_pact;
+	std::vector<float> m_fluid, m_solid, m_vel[3], m_svel[3], m_dens[3], m_p;
+	std::vector<uint8_t> m_fluid_active, m_solid_active, m_vact[3], m_svact[3], m_dact[3], m_pact;
 };
 //
 extern "C" module * create_instance() {

@@ -9,8 +9,15 @@ src/projection/macpressuresolver3.cpp):
   ``SecondOrderAccurateFluid``, ``SecondOrderAccurateSolid``) plus ``B200.*``
   keys for the device solver;
 * ``initialize(shape, dx)`` as the private initialize the module receives;
-* ``project(dt, velocity, solid, solid_velocity, fluid)`` updates the face
-  velocities (values and active bits) in place and keeps the pressure;
+* ``project(dt, velocity, solid, solid_velocity, fluid, surface_tension)``
+  updates the face velocities (values and active bits) in place and keeps
+  the pressure;
+* ``set_target_volume(current, target)`` and ``set_solid_density(density)``
+  as the interface's setters; ``Gain``, ``WarmStart`` and ``TileSize`` (the
+  grids' tile edge, which numbers the warm-start vector) are read like the
+  reference module reads them;
+* ``serialize()`` / ``initialize_from(state)`` carry the fields the module
+  serialises (macpressuresolver3.cpp:320-342);
 * ``get_pressure()`` returns the pressure grid.
 
 Grids are ``Grid`` (``array3``: values as the reference reads them plus active
@@ -63,6 +70,8 @@ class MacPressureSolver3:
         self.pressure: Optional[Grid] = None
         self.last_result: Optional[dict] = None
         self._ctx: Optional[native.Context] = None
+        self.solid_density: Optional[list] = None
+        self._volume = [0.0, 0.0, 0.0]  # target, current, y_prev
         if config:
             self.configure(config)
 
@@ -89,26 +98,92 @@ class MacPressureSolver3:
         c.stall_window = int(g("B200.StallWindow", c.stall_window))
         c.device = int(g("B200.Device", c.device))
         c.mic_block = int(g("B200.MICBlock", c.mic_block))
+        c.gain = float(g("Gain", c.gain))
+        c.warm_start = int(bool(g("WarmStart", c.warm_start)))
+        c.index_tile = int(g("TileSize", c.index_tile))
         if self._ctx is not None:
             self._ctx.set_config(c)
 
     def initialize(self, shape, dx: float) -> None:
         self.shape = tuple(int(s) for s in shape)
         self.dx = float(dx)
+        self.post_initialize()
+
+    def post_initialize(self) -> None:
         nx, ny, nz = self.shape
         self.pressure = Grid.zeros((nz, ny, nx))
+        self._volume = [0.0, 0.0, 0.0]
+        if self._ctx is not None:
+            self._push_volume()
+
+    def set_target_volume(self, current_volume: float, target_volume: float) -> None:
+        if self._ctx is not None:
+            self._pull_volume()  # keep the controller state (y_prev) the projections advanced
+        self._volume[0] = float(target_volume)
+        self._volume[1] = float(current_volume)
+        self._push_volume()
+
+    def set_solid_density(self, density) -> None:
+        """Per-face solid density: a MacGrid, three face arrays, or None."""
+        if density is None:
+            self.solid_density = None
+            return
+        vals = density.values if isinstance(density, MacGrid) else density
+        self.solid_density = [np.ascontiguousarray(v, np.float32) for v in vals]
+
+    def _push_volume(self) -> None:
+        st = (ctypes.c_double * 3)(*self._volume)
+        self.context.check(native.load().shkz_b200_set_volume_state(self.context.handle, st), "set_volume_state")
+
+    def _pull_volume(self) -> None:
+        st = (ctypes.c_double * 3)()
+        self.context.check(native.load().shkz_b200_get_volume_state(self.context.handle, st), "get_volume_state")
+        self._volume = list(st)
+
+    def warm_start_vector(self) -> np.ndarray:
+        """The previous solution by unknown number (m_prev_pressure)."""
+        L = native.load()
+        n = L.shkz_b200_warm_start_size(self.context.handle)
+        out = np.zeros(max(0, n), np.float64)
+        self.context.check(L.shkz_b200_get_warm_start(self.context.handle, out.ctypes.data, out.size),
+                           "get_warm_start")
+        return out
+
+    def set_warm_start_vector(self, prev: np.ndarray) -> None:
+        prev = np.ascontiguousarray(prev, np.float64)
+        self.context.check(native.load().shkz_b200_set_warm_start(self.context.handle, prev.ctypes.data, prev.size),
+                           "set_warm_start")
+
+    def serialize(self) -> dict:
+        """shape, dx, target/current volume, y_prev and (with WarmStart) the
+        previous solution, as macpressuresolver3::serialize writes them."""
+        self._pull_volume()
+        st = {"shape": self.shape, "dx": self.dx, "target_volume": self._volume[0],
+              "current_volume": self._volume[1], "y_prev": self._volume[2]}
+        if self.cfg.warm_start:
+            st["prev_pressure"] = self.warm_start_vector()
+        return st
+
+    def initialize_from(self, st: dict) -> None:
+        self.shape = tuple(st["shape"])
+        self.dx = float(st["dx"])
+        nx, ny, nz = self.shape
+        self.pressure = Grid.zeros((nz, ny, nx))
+        self._volume = [float(st["target_volume"]), float(st["current_volume"]), float(st["y_prev"])]
+        self._push_volume()
+        if self.cfg.warm_start and "prev_pressure" in st:
+            self.set_warm_start_vector(st["prev_pressure"])
 
     @property
     def context(self) -> native.Context:
         if self._ctx is None:
             self._ctx = native.Context(self.cfg)
+            self._push_volume()
         return self._ctx
 
     # -- macproject3_interface ------------------------------------------
     def project(self, dt: float, velocity: MacGrid, solid: Optional[Grid], solid_velocity: Optional[MacGrid],
                 fluid: Grid, surface_tension: float = 0.0, rigidbodies=None) -> dict:
-        if surface_tension:
-            raise NotImplementedError("surface tension is not supported by the B200 projection")
         if self.shape is None:
             raise RuntimeError("initialize(shape, dx) must be called before project()")
         nx, ny, nz = self.shape
@@ -132,6 +207,11 @@ class MacPressureSolver3:
                 sv, p = _c(solid_velocity.values[d], np.float32)
                 keep.append(sv)
                 args.solid_velocity[d] = p.value
+        args.surface_tension = float(surface_tension)
+        if self.solid_density is not None:
+            for d in range(3):
+                keep.append(self.solid_density[d])
+                args.solid_density[d] = self.solid_density[d].ctypes.data
         pressure = np.zeros((nz, ny, nx), np.float32)
         pact = np.zeros((nz, ny, nx), np.uint8)
         args.pressure = pressure.ctypes.data

@@ -16,8 +16,13 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "slow: long-running")
 
 
-def golden_names():
-    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz"))
+def golden_names(prefix: str = ""):
+    """Fixtures of plain projections, or (prefix "term_") of projections with
+    one optional term on."""
+    names = sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz"))
+    if prefix:
+        return [n for n in names if n.startswith(prefix)]
+    return [n for n in names if not n.startswith("term_")]
 
 
 def load_golden(name):
@@ -55,3 +60,24 @@ class GoldenScene:
 @pytest.fixture(params=golden_names() if os.path.isdir(GOLDEN) else [])
 def golden(request):
     return request.param, load_golden(request.param)
+
+
+@pytest.fixture(params=golden_names("term_") if os.path.isdir(GOLDEN) else [])
+def golden_term(request):
+    return request.param, load_golden(request.param)
+
+
+def term_options(g):
+    """Keyword options of oracle.project / the B200 solver for a term_ fixture."""
+    opt = {}
+    if float(g["kappa"]):
+        opt["kappa"] = float(g["kappa"])
+    if "density_u" in g:
+        opt["density"] = [g["density_u"], g["density_v"], g["density_w"]]
+    if float(g["volume"][1]):
+        opt["volume"] = (float(g["volume"][0]), float(g["volume"][1]), 0.0, float(g["gain"]))
+    if int(g["warm_start"]):
+        opt["warm_start"] = True
+    opt["tile"] = int(g["tile"])
+    opt["repeat"] = int(g["repeat"])
+    return opt

@@ -66,11 +66,77 @@ def make(name: str, build) -> str:
     return path
 
 
+# Optional terms of the projection (macpressuresolver3.cpp:75-80, 98-128,
+# 219-259, 286-293): each case runs the reference's MIC(0) mode with one term on.
+def _density(sc, seed):
+    rng = np.random.default_rng(seed)
+    shapes = [(sc.nz, sc.ny, sc.nx + 1), (sc.nz, sc.ny + 1, sc.nx), (sc.nz + 1, sc.ny, sc.nx)]
+    return [rng.uniform(0.0, 1.0, s).astype(np.float32) for s in shapes]
+
+
+TERM_CASES = {
+    "term_surface_tension_20": lambda: (scenes.training_scene(n=20, seed=5), {"kappa": 0.05}),
+    "term_solid_density_20": lambda: (scenes.dambreak_sphere(n=20, seed=2), {"density_seed": 17}),
+    "term_volume_correction_20": lambda: (scenes.sloshing_tank(n=20, seed=2, tol=1e-6),
+                                          {"volume": (1.05, 1.0), "gain": 1.0}),
+    "term_warm_start_20": lambda: (scenes.training_scene(n=20, seed=9), {"warm_start": True, "tile": 16}),
+}
+
+
+def make_term(name: str, build) -> str:
+    sc, opt = build()
+    extra, density, tile, repeat = {}, None, 8, 1
+    if "kappa" in opt:
+        extra["HarnessSurfaceTension"] = repr(opt["kappa"])
+    if "density_seed" in opt:
+        density = _density(sc, opt["density_seed"])
+    if "volume" in opt:
+        extra["HarnessVolume"] = "%r:%r" % opt["volume"]
+        extra["Gain"] = repr(opt["gain"])
+    if opt.get("warm_start"):
+        extra["WarmStart"] = "Yes"
+        tile, repeat = opt["tile"], 2
+    r = ref_runner.run_reference(sc, mode="mic0", tile_size=tile, repeat=repeat, extra=extra, density=density)
+    payload = dict(
+        shape=np.array([sc.nx, sc.ny, sc.nz], np.int32),
+        dx=np.float64(sc.dx), dt=np.float64(sc.dt), tol=np.float64(sc.tol),
+        fluid=r.fluid.astype(np.float32), fluid_active=r.fluid_active,
+        solid=r.solid.astype(np.float32), solid_active=r.solid_active,
+        has_solid=np.int32(sc.solid_phi is not None),
+        u_in=r.velocity_in[0].astype(np.float32), v_in=r.velocity_in[1].astype(np.float32),
+        w_in=r.velocity_in[2].astype(np.float32),
+        u_in_active=r.velocity_in_active[0], v_in_active=r.velocity_in_active[1],
+        w_in_active=r.velocity_in_active[2],
+        pressure=r.pressure.astype(np.float32), pressure_active=r.pressure_active,
+        u=r.velocity[0].astype(np.float32), v=r.velocity[1].astype(np.float32), w=r.velocity[2].astype(np.float32),
+        u_active=r.velocity_active[0], v_active=r.velocity_active[1], w_active=r.velocity_active[2],
+        iterations_mic0=np.int32(r.iterations), reresid_mic0=np.float64(r.reresid),
+        rhs=r.system["rhs"], kappa=np.float64(opt.get("kappa", 0.0)),
+        volume=np.array(opt.get("volume", (0.0, 0.0)), np.float64), gain=np.float64(opt.get("gain", 1.0)),
+        warm_start=np.int32(bool(opt.get("warm_start"))), tile=np.int32(tile), repeat=np.int32(repeat),
+    )
+    if density is not None:
+        payload.update(density_u=density[0], density_v=density[1], density_w=density[2])
+    svel = sc.solid_velocity_effective()
+    payload.update(us=svel[0], vs=svel[1], ws=svel[2])
+    path = os.path.join(OUT, f"{name}.npz")
+    np.savez_compressed(path, **payload)
+    return path
+
+
 def main():
     if not ref_runner.ref_available("float"):
         raise SystemExit("compiled reference not found: run `make -C oracle/ref` first")
+    only = sys.argv[1:]
     for name, build in CASES.items():
+        if only and name not in only:
+            continue
         p = make(name, build)
+        print(p, os.path.getsize(p))
+    for name, build in TERM_CASES.items():
+        if only and name not in only:
+            continue
+        p = make_term(name, build)
         print(p, os.path.getsize(p))
 
 

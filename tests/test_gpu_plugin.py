@@ -34,3 +34,34 @@ def test_plugin_matches_reference_module(n, seed):
     for d in range(3):
         np.testing.assert_array_equal(got.velocity_active[d], ref.velocity_active[d])
         assert rel_inf(got.velocity[d], ref.velocity[d]) <= 1e-5
+
+
+@pytest.mark.skipif(not (ref_runner.ref_available("float") and os.path.exists(PLUGIN)),
+                    reason="needs the compiled reference harness and the plugin (built where the reference is mounted)")
+@pytest.mark.parametrize("term", ["surface_tension", "solid_density", "volume_correction", "warm_start"])
+def test_plugin_optional_terms(term):
+    """Each optional term through the module loader, against the reference module
+    with the same harness keys."""
+    sc = scenes.training_scene(n=24, seed=13) if term != "solid_density" else scenes.dambreak_sphere(n=24, seed=5)
+    extra, density, tile, repeat = {}, None, 8, 1
+    if term == "surface_tension":
+        extra["HarnessSurfaceTension"] = "0.05"
+    elif term == "solid_density":
+        rng = np.random.default_rng(3)
+        density = [rng.uniform(0, 1, s).astype(np.float32) for s in
+                   [(sc.nz, sc.ny, sc.nx + 1), (sc.nz, sc.ny + 1, sc.nx), (sc.nz + 1, sc.ny, sc.nx)]]
+    elif term == "volume_correction":
+        extra.update({"HarnessVolume": "0.9:1.0", "Gain": "1.0"})
+    else:
+        extra["WarmStart"] = "Yes"
+        tile, repeat = 16, 2
+    ref = ref_runner.run_reference(sc, mode="mic0", dump_system=False, tile_size=tile, repeat=repeat, extra=extra,
+                                   density=density)
+    got = ref_runner.run_reference(sc, mode="mic0", dump_system=False, tile_size=tile, repeat=repeat,
+                                   extra=dict(extra, Projection="macpressuresolver3_b200"), extra_libpath=[PKG],
+                                   density=density)
+    np.testing.assert_array_equal(got.pressure_active, ref.pressure_active)
+    assert rel_inf(got.pressure, ref.pressure) <= 1e-5
+    for d in range(3):
+        np.testing.assert_array_equal(got.velocity_active[d], ref.velocity_active[d])
+        assert rel_inf(got.velocity[d], ref.velocity[d]) <= 1e-5
