@@ -170,9 +170,14 @@ int shkz_b200_project_device(shkz_b200_ctx *ctx, const shkz_b200_project_args *a
  * can order their own work against it. */
 void *shkz_b200_stream(shkz_b200_ctx *ctx);
 
-/* Generic solver path for LinSolver=: solves A x = b for a symmetric CSR
- * matrix given on the host (row-sorted, 0-based, FP64), same stopping rule
- * as the reference PCG, MIC(0) computed on the device from the CSR. */
+/* Generic solver path for LinSolver= (replaces pcg_solver::solve,
+ * src/linsolver/pcg.cpp:45-73): solves A x = b for a symmetric CSR matrix
+ * given on the host (row-sorted, 0-based, FP64) with the algorithm the
+ * reference's pcg module runs as shipped -- conjugate gradients with the
+ * identity preconditioner (its MIC(0) result is overwritten,
+ * local/include/pcgsolver/pcg_solver.h:379-384), x0 = 0, stop at
+ * ||r||inf <= residual * ||b||inf, iterations = iteration + 1 -- in FP64 on
+ * the device. The config's preconditioner field is not used here. */
 int shkz_b200_solve_csr(shkz_b200_ctx *ctx, long long n, const long long *indptr, const long long *indices,
                         const double *data, const double *b, double *x, shkz_b200_result *out);
 

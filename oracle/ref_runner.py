@@ -10,6 +10,7 @@ from __future__ import annotations
 
 import dataclasses
 import os
+import re
 import struct
 import subprocess
 import tempfile
@@ -39,6 +40,7 @@ class RefResult:
     velocity_active: list
     projection_ms: float
     iterations: Optional[int] = None
+    console_solves: list = dataclasses.field(default_factory=list)
     reresid: Optional[float] = None
     solve_ms: Optional[float] = None
     system: Optional[dict] = None
@@ -104,11 +106,14 @@ def run_reference(scene, variant: str = "float", mode: str = "mic0", tol: Option
             p, pm = _read_cells(f, cs)
             vout = [_read_cells(f, s) for s in fs]
             ms = struct.unpack("<d", f.read(8))[0]
+        # the reference module's own console line per solve: "Took N iterations, Reresid=X"
+        solves = re.findall(r"Took (\d+) iterations, Reresid=([-+]?(?:nan|inf|[0-9]+(?:\.[0-9]*)?(?:[eE][-+]?[0-9]+)?))", proc.stdout)
         res = RefResult(fluid=fluid, fluid_active=fluid_m, solid=solid, solid_active=solid_m,
                         velocity_in=[v for v, _ in vin], velocity_in_active=[m for _, m in vin],
                         pressure=p, pressure_active=pm,
                         velocity=[v for v, _ in vout], velocity_active=[m for _, m in vout],
-                        projection_ms=ms)
+                        projection_ms=ms,
+                        console_solves=[(int(a), float(b)) for a, b in solves])
         if dump_system and os.path.exists(dump + ".solve.txt"):
             it, rr, sms = open(dump + ".solve.txt").read().split()
             res.iterations, res.reresid, res.solve_ms = int(it), float(rr), float(sms)

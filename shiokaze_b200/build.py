@@ -62,7 +62,8 @@ def build(verbose: bool = False, extra=None) -> str:
     return LIB
 
 
-PLUGINS = {"libshiokaze_macpressuresolver3_b200.so": "macpressuresolver3_b200.cpp"}
+PLUGINS = {"libshiokaze_macpressuresolver3_b200.so": "macpressuresolver3_b200.cpp",
+           "libshiokaze_pcg_b200.so": "pcg_b200.cpp"}
 
 
 def build_plugins(reference_root: str, verbose: bool = False) -> list:

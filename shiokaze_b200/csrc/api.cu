@@ -1013,7 +1013,6 @@ extern "C" int shkz_b200_solve_csr(shkz_b200_ctx *ctx, long long n, const long l
   if (n == 0) return 0;
   const long long nnz = indptr[n];
   if (n > INT32_MAX || nnz > INT32_MAX) return res->status = SHKZ_B200_ERR_LIMIT;
-  if (ctx->cfg.preconditioner != SHKZ_B200_PRECOND_NONE) return res->status = SHKZ_B200_ERR_ARG;
   cudaSetDevice(ctx->device);
   cudaStream_t s = ctx->stream;
   std::vector<int> hp((size_t)n + 1), hi((size_t)nnz);

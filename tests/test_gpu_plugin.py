@@ -65,3 +65,27 @@ def test_plugin_optional_terms(term):
     for d in range(3):
         np.testing.assert_array_equal(got.velocity_active[d], ref.velocity_active[d])
         assert rel_inf(got.velocity[d], ref.velocity[d]) <= 1e-5
+
+
+PCG_PLUGIN = os.path.join(PKG, "libshiokaze_pcg_b200.so")
+
+
+@pytest.mark.skipif(not (ref_runner.ref_available("float") and os.path.exists(PCG_PLUGIN)),
+                    reason="needs the compiled reference harness and the pcg_b200 module")
+@pytest.mark.parametrize("n,seed,tol", [(24, 1, 1e-4), (32, 2, 1e-6)])
+def test_pcg_b200_matches_reference_pcg(n, seed, tol):
+    """The reference's own macpressuresolver3 with LinSolver=pcg_b200 (our module,
+    loaded by the reference's loader) against LinSolver=pcg (the reference's)."""
+    sc = scenes.dambreak_sphere(n=n, seed=seed, tol=tol)
+    ref = ref_runner.run_reference(sc, linsolver="pcg", dump_system=False)
+    got = ref_runner.run_reference(sc, linsolver="pcg_b200", dump_system=False, extra_libpath=[PKG])
+    (it_ref, rr_ref), (it_got, rr_got) = ref.console_solves[-1], got.console_solves[-1]
+    # unpreconditioned CG: summation order alone moves the stop by 3-5 %
+    assert abs(it_got - it_ref) <= max(2, int(0.05 * it_ref)), (it_got, it_ref)
+    assert rr_got <= tol
+    tol_p = max(1e-5, 10 * tol)
+    np.testing.assert_array_equal(got.pressure_active, ref.pressure_active)
+    assert rel_inf(got.pressure, ref.pressure) <= tol_p
+    for d in range(3):
+        np.testing.assert_array_equal(got.velocity_active[d], ref.velocity_active[d])
+        assert rel_inf(got.velocity[d], ref.velocity[d]) <= tol_p
