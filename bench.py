@@ -48,6 +48,19 @@ ALGO_BYTES = {
 }
 
 
+def job_ms_per_projection(elapsed_ms: float, steps: int, world: int, device=None) -> float:
+    """Whole-job ms per projection: the slowest rank's timed region (max over
+    ranks, all_reduce MAX) over the projections all ranks ran. Replicas run
+    independent projections, so per-rank work is fixed as ranks are added."""
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([elapsed_ms], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+    return elapsed_ms / (steps * world)
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -197,7 +210,11 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--mic-block", type=int, default=16, choices=[8, 16],
                     help="MIC(0) sweep block edge (16: 2x2x2 tiles per CTA)")
-    ap.add_argument("--model", default=None, help="trained network for --precond learned")
+    ap.add_argument("--model", default=None, help="trained network for the learned preconditioner")
+    ap.add_argument("--scene", default="sloshing_tank", choices=["sloshing_tank", "splash", "dambreak_rain"],
+                    help="sloshing_tank 256^3 (headline), splash 384^3, dambreak_rain 512^3")
+    ap.add_argument("--learned-steps", type=int, default=2,
+                    help="timed projections of the learned-preconditioner arm (0: skip)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -216,7 +233,12 @@ def main():
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
 
-    sc = scenes.sloshing_tank(n=args.n, seed=0, tol=1e-6)
+    if args.scene == "sloshing_tank":
+        sc = scenes.sloshing_tank(n=args.n, seed=0, tol=1e-6)
+    elif args.scene == "splash":
+        sc = scenes.splash(n=args.n if args.n != 256 else 384, seed=0, tol=1e-6)
+    else:
+        sc = scenes.dambreak_rain(n=args.n if args.n != 256 else 512, seed=0, tol=1e-6)
     nx, ny, nz = sc.nx, sc.ny, sc.nz
 
     cfg = native.default_config()
@@ -287,13 +309,7 @@ def main():
         torch.cuda.synchronize(dev)
     if world > 1:
         dist.barrier()
-    elapsed_ms = ev0.elapsed_time(ev1)
-    t = torch.tensor([elapsed_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    elapsed_ms = float(t.item())
-    total_proj = args.steps * world
-    value = elapsed_ms / total_proj if world > 1 else elapsed_ms / args.steps
+    value = job_ms_per_projection(ev0.elapsed_time(ev1), args.steps, world, dev)
     clocks = clk.summary()
     last = results[-1]
 
@@ -314,19 +330,36 @@ def main():
             entry["achieved_gbs"] = gbs
         kern[name] = entry
     peak, peak_kind = measured_peaks()
-    sp = kern.get("spmv", {})
-    traffic = ncu_traffic()
-    traffic_bytes = None
-    if traffic and "spmv" in traffic and sp.get("cells"):
-        t0 = traffic["spmv"]
-        traffic_bytes = t0["dram_bytes_per_launch"] * sp["cells"] / t0["cells"]
+    traffic = ncu_traffic() or {}
+    names = {"spmv": "k_spmv (7-point stencil q = A p with fused p.q)",
+             "mic_sweeps": "k_mic_forward16 + k_mic_backward16 (MIC(0) wavefront sweeps, fused z.r)",
+             "update_xr": "k_update_xr (x, r update with inf/2-norms)", "update_p": "k_update_p"}
+    rooflines = {}
+    for kname, entry in kern.items():
+        if "achieved_gbs" not in entry:
+            continue
+        tb = None
+        if kname in traffic and entry.get("cells"):
+            t0 = traffic[kname]
+            tb = t0["dram_bytes_per_launch"] * entry["cells"] / t0["cells"]
+        rooflines[kname] = {"kernel": names.get(kname, kname), "bound": "hbm", "achieved": entry["achieved_gbs"],
+                            "peak": peak, "unit": "GB/s", "frac": entry["achieved_gbs"] / peak,
+                            "peak_kind": peak_kind, "ms": entry["ms"],
+                            "algo_bytes_per_launch": ALGO_BYTES[kname] * entry["cells"], "traffic": tb}
+    # the dominant kernel of an iteration by device time
     roofline = None
-    if "achieved_gbs" in sp:
-        roofline = {"kernel": "k_spmv (7-point stencil q = A p with fused p.q)", "bound": "hbm",
-                    "achieved": sp["achieved_gbs"], "peak": peak, "unit": "GB/s",
-                    "frac": sp["achieved_gbs"] / peak, "peak_kind": peak_kind,
-                    "algo_bytes_per_launch": ALGO_BYTES["spmv"] * sp["cells"],
-                    "traffic": traffic_bytes}
+    if rooflines:
+        dom = max(rooflines, key=lambda k: rooflines[k]["ms"])
+        roofline = dict(rooflines[dom])
+        if dom == "mic_sweeps":
+            roofline["note"] = ("wavefront-latency bound: 48 dependent macro-tile levels per sweep at 256^3; "
+                                "the HBM fraction shows how far the dependency chain keeps it from streaming")
+    ms_it = last["ms_solve"] / max(1, last["iterations"])
+    it_bytes = sum(ALGO_BYTES.values()) * kern.get("spmv", {}).get("cells", 0)
+    iteration_roofline = {"bytes_per_iteration": it_bytes, "ms_per_iteration": ms_it,
+                          "achieved": it_bytes / (ms_it * 1e-3) / 1e9 if ms_it else None, "peak": peak,
+                          "unit": "GB/s", "frac": (it_bytes / (ms_it * 1e-3) / 1e9) / peak if ms_it else None,
+                          "algo_bytes_per_cell": sum(ALGO_BYTES.values())}
 
     # end to end through the host-buffer C-ABI call with pinned host memory
     e2e = None
@@ -368,6 +401,46 @@ def main():
                "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
                "h2d_ms": hres.ms_h2d, "d2h_ms": hres.ms_d2h}
 
+    # error against the FP64 tight-tolerance solve on the device (untimed)
+    fp64 = None
+    if rank == 0:
+        cfg.fp64_reference = 1
+        ctx.set_config(cfg)
+        r64 = step()
+        fp64 = {"err_inf_vs_fp64": r64["err_fp64_inf"], "fp64_reresid": r64["fp64_reresid"]}
+        cfg.fp64_reference = 0
+        ctx.set_config(cfg)
+
+    # learned-preconditioner arm on the same device inputs: flexible PCG with
+    # the trained network, MIC(0) fallback on stall
+    learned = None
+    model = args.model or DEFAULT_MODEL
+    if rank == 0 and args.precond == "mic0" and args.learned_steps > 0 and os.path.exists(model):
+        try:
+            ctx.check(L.shkz_b200_learned_load(ctx.handle, model.encode()), "shkz_b200_learned_load")
+            cfg.preconditioner = native.PRECOND_LEARNED
+            ctx.set_config(cfg)
+            step()  # warm-up (network block activity of this system)
+            torch.cuda.synchronize(dev)
+            la, lb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            lres = []
+            la.record(stream)
+            for _ in range(args.learned_steps):
+                lres.append(step())
+            lb.record(stream)
+            torch.cuda.synchronize(dev)
+            lms = la.elapsed_time(lb) / args.learned_steps
+            ll = lres[-1]
+            learned = {"ms_per_projection": lms, "iterations": ll["iterations"], "fallbacks": ll["fallbacks"],
+                       "reresid_inf": ll["reresid"], "ms_solve": ll["ms_solve"], "status": ll["status"],
+                       "model": os.path.relpath(model, ROOT), "steps": args.learned_steps,
+                       "plain_ms_per_projection": value, "plain_iterations": last["iterations"],
+                       "speedup_vs_plain": value / lms if lms else None}
+        except native.ShkzError as exc:  # reported in the line, not hidden
+            learned = {"error": str(exc), "model": os.path.relpath(model, ROOT)}
+        cfg.preconditioner = native.PRECOND_MIC0
+        ctx.set_config(cfg)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -380,18 +453,20 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": value, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 (f64 reductions, refinement and assembly)", "data": "synthetic",
-            "config": {"workload": f"sloshing_tank {nx}^3, plain MIC(0)-PCG projection to 1e-6 (inf-norm), "
-                                   f"FP64 refinement, seed 0", "preconditioner": args.precond,
+            "config": {"workload": f"{args.scene} {nx}^3, {'plain MIC(0)' if args.precond == 'mic0' else args.precond}"
+                                   f"-PCG projection to 1e-6 (inf-norm), FP64 refinement, seed 0",
+                       "preconditioner": args.precond,
                        "unknowns": last["unknowns"], "pool_tiles": last["tiles"],
-                       "l2": "inputs 0.42 GB and pool arrays > 126 MB L2 (no flush needed)",
+                       "l2": "inputs (0.42 GB at 256^3) and pool arrays > 126 MB L2 (no flush needed)",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "step": "device velocity restore + one projection"},
             "iterations": last["iterations"], "outer_steps": last["outer_steps"],
             "reresid_inf": last["reresid"], "reresid_l2": last["reresid_l2"],
             "phase_ms": {"assemble": last["ms_assemble"], "solve": last["ms_solve"], "update": last["ms_update"]},
             "ms_per_iteration": last["ms_solve"] / max(1, last["iterations"]),
-            "e2e": e2e, "roofline": roofline, "kernels": kern, "cpu_baseline": cpu, "clocks": clocks,
-            "gpu_launches": launches,
+            "e2e": e2e, "roofline": roofline, "roofline_kernels": rooflines, "roofline_iteration": iteration_roofline,
+            "error_vs_fp64": fp64, "learned": learned,
+            "kernels": kern, "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -500,11 +500,14 @@ __global__ void k_adam(float *w, const float *g, float *m, float *v, int n, floa
   }
 }
 
-// dL/dZ for the energy loss 1/2 z.A z - z.r (z, r scaled): q = A z - r at unknowns,
-// scattered into the dense FP32 gradient of the output; also the loss terms.
-// gradient gscale (A z - r) and energy gscale (1/2 z.Az - z.r) of the output
+// Scale-invariant energy loss: L(z) = g E(c z) with E(y) = 1/2 y.A y - y.r
+// and c = z.r / z.A z the best step along z, i.e. -g/2 (z.r)^2 / z.A z, the
+// energy a conjugate-direction step along z removes. Its gradient is
+// dL/dz = g c (c A z - r); it does not reward shrinking z, which the plain
+// energy does while the output is still uncorrelated with the error. Writes
+// the gradient into the dense FP32 output gradient and the loss terms.
 __global__ void k_energy_grad(Geometry G, int NX, int NY, const int *pool_tile, int K, const uint8_t *unk,
-                              const float *Az, const float *zp, const float *rp, float gscale, float *gZ,
+                              const float *Az, const float *zp, const float *rp, float cz, float gscale, float *gZ,
                               double *partials) {
   __shared__ double red[8];
   double e = 0.0;
@@ -516,12 +519,28 @@ __global__ void k_energy_grad(Geometry G, int NX, int NY, const int *pool_tile, 
               z = (int)(t / ((long long)G.bx * G.by)) * 8 + (c >> 6);
     if (x >= G.nx || y >= G.ny || z >= G.nz) continue;
     if (!unk[(size_t)x + (size_t)G.nx * ((size_t)y + (size_t)G.ny * z)]) continue;
-    const float q = Az[o] - rp[o];
+    const float q = cz * Az[o] - rp[o];
     gZ[((size_t)z * NY + y) * NX + x] = gscale * q;
-    e += 0.5 * (double)zp[o] * Az[o] - (double)zp[o] * rp[o];
+    e += 0.5 * (double)cz * cz * zp[o] * Az[o] - (double)cz * zp[o] * rp[o];
   }
-  e = block_sum<256>(e, red) * (double)gscale;
+  e = block_sum<256>(e, red);
   if (threadIdx.x == 0) partials[blockIdx.x] = e;
+}
+
+// z.r and z.A z over the pool (both zero outside unknowns)
+__global__ void k_dot2_pool(size_t n, const float *z, const float *r, const float *Az, double *partials) {
+  __shared__ double red[8];
+  double a = 0.0, b = 0.0;
+  for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < n; o += (size_t)gridDim.x * blockDim.x) {
+    a += (double)z[o] * r[o];
+    b += (double)z[o] * Az[o];
+  }
+  a = block_sum<256>(a, red);
+  b = block_sum<256>(b, red);
+  if (threadIdx.x == 0) {
+    partials[2 * blockIdx.x] = a;
+    partials[2 * blockIdx.x + 1] = b;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1092,11 +1111,24 @@ int learned_train_step(LearnedModel *m, const LearnedSystem &sys, const PoolSyst
   int rc = learned_apply(m, sys, r_pool, 1.0, z_pool, s);
   if (rc) return rc;
   launch_spmv(S, z_pool, Az_pool, partials, counter, nullptr, 1, s);
-  cudaMemsetAsync(m->gZ, 0, nvox(m, 0) * 4, s);
   const int nb = 148 * 4;
+  // best step c along z (plain energy gradient while z.A z is not yet positive)
+  std::vector<double> hd(2 * nb);
+  count_launches(1);
+  k_dot2_pool<<<nb, 256, 0, s>>>((size_t)sys.K * SHKZ_TC, z_pool, r_pool, Az_pool, m->partials);
+  if (cudaMemcpyAsync(hd.data(), m->partials, sizeof(double) * 2 * nb, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return SHKZ_B200_ERR_CUDA;
+  double zr = 0.0, zaz = 0.0;
+  for (int i = 0; i < nb; ++i) {
+    zr += hd[2 * i];
+    zaz += hd[2 * i + 1];
+  }
+  const double c = (zaz > 0.0 && zaz < 1e300 && zr == zr) ? zr / zaz : 1.0;
+  cudaMemsetAsync(m->gZ, 0, nvox(m, 0) * 4, s);
   count_launches(1);
   k_energy_grad<<<nb, 256, 0, s>>>(sys.G, m->NX[0], m->NY[0], sys.pool_tile, sys.K, sys.unk, Az_pool, z_pool, r_pool,
-                                   (float)gscale, m->gZ, m->partials);
+                                   (float)c, (float)(gscale * c), m->gZ, m->partials);
   std::vector<double> hp(nb);
   cudaMemcpyAsync(hp.data(), m->partials, sizeof(double) * nb, cudaMemcpyDeviceToHost, s);
   rc = backward(m, s);
@@ -1106,7 +1138,7 @@ int learned_train_step(LearnedModel *m, const LearnedSystem &sys, const PoolSyst
   if (cudaStreamSynchronize(s) != cudaSuccess) return SHKZ_B200_ERR_CUDA;
   double e = 0.0;
   for (double v : hp) e += v;
-  if (loss) *loss = e;
+  if (loss) *loss = e * gscale;
   int herr = 0;
   cudaMemcpy(&herr, m->err, sizeof(int), cudaMemcpyDeviceToHost);
   return herr ? SHKZ_B200_ERR_TIMEOUT : 0;
