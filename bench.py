@@ -259,8 +259,9 @@ def main():
         return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
     fluid = dev_t(sc.fluid_effective(), np.float32)
     fact = dev_t(sc.fluid_active.astype(np.uint8), np.uint8)
-    solid = dev_t(sc.solid_effective(), np.float32)
-    sact = dev_t(sc.solid_active.astype(np.uint8), np.uint8)
+    has_solid = sc.solid_phi is not None
+    solid = dev_t(sc.solid_effective(), np.float32) if has_solid else None
+    sact = dev_t(sc.solid_active.astype(np.uint8), np.uint8) if has_solid else None
     vel0 = [dev_t(v, np.float32) for v in sc.velocity_effective()]
     vact0 = [dev_t(m.astype(np.uint8), np.uint8) for m in sc.velocity_active]
     vel = [v.clone() for v in vel0]
@@ -272,7 +273,8 @@ def main():
     a = native.ProjectArgs()
     a.nx, a.ny, a.nz, a.dx, a.dt = nx, ny, nz, sc.dx, sc.dt
     a.fluid, a.fluid_active = fluid.data_ptr(), fact.data_ptr()
-    a.solid, a.solid_active = solid.data_ptr(), sact.data_ptr()
+    if has_solid:
+        a.solid, a.solid_active = solid.data_ptr(), sact.data_ptr()
     for d in range(3):
         a.velocity[d] = vel[d].data_ptr()
         a.velocity_active[d] = vact[d].data_ptr()
@@ -366,7 +368,8 @@ def main():
     if rank == 0 or world > 1:
         pin = lambda arr: torch.from_numpy(np.ascontiguousarray(arr)).pin_memory()
         h_fluid, h_fact = pin(sc.fluid_effective()), pin(sc.fluid_active.astype(np.uint8))
-        h_solid, h_sact = pin(sc.solid_effective()), pin(sc.solid_active.astype(np.uint8))
+        h_solid = pin(sc.solid_effective()) if has_solid else None
+        h_sact = pin(sc.solid_active.astype(np.uint8)) if has_solid else None
         h_vel0 = [v.copy() for v in sc.velocity_effective()]
         h_vact0 = [m.astype(np.uint8).copy() for m in sc.velocity_active]
         h_vel = [pin(v) for v in h_vel0]
@@ -376,13 +379,14 @@ def main():
         ha = native.ProjectArgs()
         ha.nx, ha.ny, ha.nz, ha.dx, ha.dt = nx, ny, nz, sc.dx, sc.dt
         ha.fluid, ha.fluid_active = h_fluid.data_ptr(), h_fact.data_ptr()
-        ha.solid, ha.solid_active = h_solid.data_ptr(), h_sact.data_ptr()
+        if has_solid:
+            ha.solid, ha.solid_active = h_solid.data_ptr(), h_sact.data_ptr()
         for d in range(3):
             ha.velocity[d] = h_vel[d].data_ptr()
             ha.velocity_active[d] = h_vact[d].data_ptr()
             ha.solid_velocity[d] = None
         ha.pressure, ha.pressure_active = h_p.data_ptr(), h_pa.data_ptr()
-        h2d = (h_fluid.numel() * 4 + h_fact.numel() + h_solid.numel() * 4 + h_sact.numel()
+        h2d = (h_fluid.numel() * 4 + h_fact.numel() + (h_solid.numel() * 5 if has_solid else 0)
                + sum(v.numel() * 5 for v in h_vel))
         d2h = sum(v.numel() * 5 for v in h_vel) + h_p.numel() * 5
         e2e_steps = args.e2e_steps or args.steps

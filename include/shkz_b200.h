@@ -196,8 +196,8 @@ int shkz_b200_apply_preconditioner(shkz_b200_ctx *ctx, const float *r_cells, flo
 int shkz_b200_apply_matrix(shkz_b200_ctx *ctx, const float *x_cells, float *y_cells);
 
 /* Device timing of one kernel on the last projection's system: launches it
- * `reps` times on the context stream between CUDA events and stores the mean
- * milliseconds per launch. which: 0 = stencil q = A p with fused p.q,
+ * `reps` times on the context stream, each launch between CUDA events after a
+ * 256 MB write that evicts the L2, and stores the mean milliseconds per launch. which: 0 = stencil q = A p with fused p.q,
  * 1 = MIC(0) forward sweep, 2 = MIC(0) backward sweep with fused z.r,
  * 3 = fused x/r update with norms, 4 = p update, 5 = unknown labelling,
  * 6 = weights/rhs assembly, 7 = MIC(0) factor. *cells_out (may be NULL)
