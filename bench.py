@@ -47,6 +47,11 @@ ALGO_BYTES = {
     "update_p": 12,    # read z, p; write p
 }
 
+# One MIC(0)-PCG iteration as run: stencil 24, forward sweep with the fused
+# x/r update (reads r q p x d + 3 w, writes r x t: 44), backward sweep 28,
+# p update 12.
+ITER_BYTES = 108
+
 
 def job_ms_per_projection(elapsed_ms: float, steps: int, world: int, device=None) -> float:
     """Whole-job ms per projection: the slowest rank's timed region (max over
@@ -357,11 +362,11 @@ def main():
             roofline["note"] = ("wavefront-latency bound: 48 dependent macro-tile levels per sweep at 256^3; "
                                 "the HBM fraction shows how far the dependency chain keeps it from streaming")
     ms_it = last["ms_solve"] / max(1, last["iterations"])
-    it_bytes = sum(ALGO_BYTES.values()) * kern.get("spmv", {}).get("cells", 0)
+    it_bytes = ITER_BYTES * kern.get("spmv", {}).get("cells", 0)
     iteration_roofline = {"bytes_per_iteration": it_bytes, "ms_per_iteration": ms_it,
                           "achieved": it_bytes / (ms_it * 1e-3) / 1e9 if ms_it else None, "peak": peak,
                           "unit": "GB/s", "frac": (it_bytes / (ms_it * 1e-3) / 1e9) / peak if ms_it else None,
-                          "algo_bytes_per_cell": sum(ALGO_BYTES.values())}
+                          "algo_bytes_per_cell": ITER_BYTES}
 
     # end to end through the host-buffer C-ABI call with pinned host memory
     e2e = None

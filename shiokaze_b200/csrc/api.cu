@@ -226,7 +226,7 @@ static int ensure_pool(shkz_b200_ctx *ctx, int K) {
   GROW(colsum, n); GROW(dmic64, n); GROW(x64, n); GROW(r64, n); GROW(xref64, n);
   GROW(p64, n); GROW(q64, n); GROW(z64, n);
   GROW(x, n); GROW(r, n); GROW(p, n); GROW(q, n); GROW(z, n); GROW(t, n); GROW(p32, n);
-  GROW(partials, (size_t)cap + 4 * 8192);
+  GROW(partials, (size_t)2 * cap + 4 * 8192);
   GROW(wflags, (size_t)cap);
   GROW(faces_f, (size_t)cap * 3 * 64);
   GROW(faces_b, (size_t)cap * 3 * 64);
@@ -474,6 +474,14 @@ static int solve_system(shkz_b200_ctx *ctx, double tol, int precond, shkz_b200_r
   for (;;) {
     for (int b = 0; b < batch; ++b) {
       launch_spmv(S, ctx->p, ctx->q, ctx->partials, ctx->counter, ctx->st, 0, s);
+      // MIC(0) on macro tiles: the x/r update rides in the forward sweep's staging
+      if (precond == SHKZ_B200_PRECOND_MIC0 &&
+          launch_mic_apply_update(S, ctx->d32, ctx->r, ctx->t, ctx->z, ctx->partials, ctx->p, ctx->q, ctx->x,
+                                  ctx->counter + 1, ctx->st, max_it, wsync(ctx, 1), wsync(ctx, 2), s)) {
+        launch_finish_rho(ctx->partials, mic_partial_count(S), ctx->st, 0, s);
+        launch_update_p(n, ctx->z, ctx->p, ctx->st, s);
+        continue;
+      }
       launch_update_xr(n, ctx->p, ctx->q, ctx->x, ctx->r, ctx->partials, ctx->counter + 1, ctx->st, max_it, s);
       launch_iteration_tail(ctx, S, n, precond, s);
     }

@@ -811,6 +811,47 @@ __device__ __forceinline__ void macro_load5(const int *sub, const float *s0, con
     *reinterpret_cast<float4 *>(d4 + o) = a4;
   }
 }
+// Fused PCG update while staging (forward sweep of an iteration): r -= alpha q
+// and x += alpha p on the macro tile's cells, the new r staged for the sweep,
+// written back, and its inf-norm / squared 2-norm returned for this thread.
+__device__ __forceinline__ void macro_load_update(const int *sub, float *r, const float *q, const float *p, float *x,
+                                                  float alpha, const float *s1, const float *s2, const float *s3,
+                                                  const float *s4, float *d0, float *d1, float *d2, float *d3,
+                                                  float *d4, double &m, double &s2sum) {
+  for (int e = threadIdx.x; e < 8 * 128; e += blockDim.x) {
+    const int v = e & 127, st = e >> 7;
+    const int pt = sub[st];
+    const int c = v * 4;
+    const int xx = (c & 7) + (st & 1) * 8, y = ((c >> 3) & 7) + ((st >> 1) & 1) * 8, z = (c >> 6) + (st >> 2) * 8;
+    const int o = xx + 16 * y + 256 * z;
+    float4 a0 = make_float4(0.f, 0.f, 0.f, 0.f), a1 = a0, a2 = a0, a3 = a0, a4 = a0;
+    if (pt >= 0) {
+      const size_t b = (size_t)pt * (SHKZ_TC / 4) + v;
+      float4 rv = reinterpret_cast<const float4 *>(r)[b];
+      const float4 qv = reinterpret_cast<const float4 *>(q)[b];
+      const float4 pv = reinterpret_cast<const float4 *>(p)[b];
+      float4 xv = reinterpret_cast<const float4 *>(x)[b];
+      a1 = reinterpret_cast<const float4 *>(s1)[b];
+      a2 = reinterpret_cast<const float4 *>(s2)[b];
+      a3 = reinterpret_cast<const float4 *>(s3)[b];
+      a4 = reinterpret_cast<const float4 *>(s4)[b];
+      // the expressions of k_update_xr
+      xv.x += alpha * pv.x; xv.y += alpha * pv.y; xv.z += alpha * pv.z; xv.w += alpha * pv.w;
+      rv.x -= alpha * qv.x; rv.y -= alpha * qv.y; rv.z -= alpha * qv.z; rv.w -= alpha * qv.w;
+      reinterpret_cast<float4 *>(x)[b] = xv;
+      reinterpret_cast<float4 *>(r)[b] = rv;
+      m = fmax(m, fmax(fmax(fabs((double)rv.x), fabs((double)rv.y)), fmax(fabs((double)rv.z), fabs((double)rv.w))));
+      s2sum += (double)rv.x * rv.x + (double)rv.y * rv.y + (double)rv.z * rv.z + (double)rv.w * rv.w;
+      a0 = rv;
+    }
+    *reinterpret_cast<float4 *>(d0 + o) = a0;
+    *reinterpret_cast<float4 *>(d1 + o) = a1;
+    *reinterpret_cast<float4 *>(d2 + o) = a2;
+    *reinterpret_cast<float4 *>(d3 + o) = a3;
+    *reinterpret_cast<float4 *>(d4 + o) = a4;
+  }
+}
+
 __device__ __forceinline__ void macro_store(const int *sub, const float *srcs, float *dst) {
   for (int e = threadIdx.x; e < 8 * 128; e += blockDim.x) {
     const int v = e & 127, st = e >> 7;
@@ -822,9 +863,23 @@ __device__ __forceinline__ void macro_store(const int *sub, const float *srcs, f
   }
 }
 
+// With fu != null the kernel also performs the preceding x/r update of the
+// PCG iteration (k_update_xr's arithmetic and convergence bookkeeping, the
+// last CTA reducing the norms); the update's extra loads sit in the staging
+// phase, which overlaps the wait for the upstream faces.
+struct SweepUpdate {
+  const float *p, *q;
+  float *x, *r;
+  SolverState *st;
+  unsigned *counter;
+  double *part;        // [2 * KM]: per-tile inf-norm, squared 2-norm
+  int max_iterations;
+};
+
 __global__ void __launch_bounds__(256) k_mic_forward16(PoolSystem S, const float *__restrict__ d32,
                                                        const float *__restrict__ r, float *__restrict__ t,
-                                                       unsigned long long *faces, WaveSync *ws, const SolverState *st) {
+                                                       unsigned long long *faces, WaveSync *ws, const SolverState *st,
+                                                       SweepUpdate fu) {
   extern __shared__ __align__(16) float smf[];
   float *T = smf, *R = T + MTC, *Dd = R + MTC, *WX = Dd + MTC, *WY = WX + MTC, *WZ = WY + MTC;
   float *hx = WZ + MTC, *hy = hx + 256, *hz = hy + 256;
@@ -836,7 +891,20 @@ __global__ void __launch_bounds__(256) k_mic_forward16(PoolSystem S, const float
   const int tid = threadIdx.x, jj = tid & 15, kk = tid >> 4;
   if (tid < 8) sub[tid] = S.msub[mt * 8 + tid];
   __syncthreads();
-  macro_load5(sub, r, d32, S.offx, S.offy, S.offz, R, Dd, WX, WY, WZ);
+  if (fu.st) {
+    __shared__ double red[8];
+    double m = 0.0, s2 = 0.0;
+    macro_load_update(sub, fu.r, fu.q, fu.p, fu.x, (float)fu.st->alpha, d32, S.offx, S.offy, S.offz, R, Dd, WX, WY,
+                      WZ, m, s2);
+    m = block_max<256>(m, red);
+    s2 = block_sum<256>(s2, red);
+    if (tid == 0) {
+      fu.part[mt] = m;
+      fu.part[S.KM + mt] = s2;
+    }
+  } else {
+    macro_load5(sub, r, d32, S.offx, S.offy, S.offz, R, Dd, WX, WY, WZ);
+  }
   {
     const int nxm = S.mnbr[mt * 6 + NB_XM], nym = S.mnbr[mt * 6 + NB_YM], nzm = S.mnbr[mt * 6 + NB_ZM];
     bool ok = true;
@@ -865,6 +933,29 @@ __global__ void __launch_bounds__(256) k_mic_forward16(PoolSystem S, const float
     face_put(f + 2 * 256 + tid, epoch, T[u + MT * v + MT * MT * 15]);
   }
   macro_store(sub, T, t);
+  if (fu.st && last_block(fu.counter)) {
+    // the convergence bookkeeping of k_update_xr, on the new residual
+    __shared__ double red2[8];
+    double mm = 0.0, ss = 0.0;
+    for (int i = tid; i < S.KM; i += 256) {
+      mm = fmax(mm, fu.part[i]);
+      ss += fu.part[S.KM + i];
+    }
+    mm = block_max<256>(mm, red2);
+    ss = block_sum<256>(ss, red2);
+    const bool nan = !(ss == ss);
+    if (tid == 0) {
+      SolverState *sw = fu.st;
+      sw->rmax = nan ? CUDART_NAN : mm;
+      sw->r2 = ss;
+      sw->iter += 1;
+      if (nan) { sw->done = 3; sw->status = -5; }
+      else if (mm <= sw->tol_abs) sw->done = 1;
+      else if (sw->iter >= fu.max_iterations) sw->done = 2;
+      else if (mm < sw->ru_threshold) sw->done = 4;
+      *fu.counter = 0;
+    }
+  }
   sweep_end(ws, epoch);
 }
 
@@ -1360,7 +1451,8 @@ void launch_mic_apply(const PoolSystem &S, const float *d32, const float *r, flo
       if (dev >= 0 && dev < 64) attr[dev] = true;
     }
     count_launches(2);
-    k_mic_forward16<<<S.KM, 256, mic16_smem_forward(), s>>>(S, d32, r, t, S.mfaces_f, (WaveSync *)ws_f, st);
+    k_mic_forward16<<<S.KM, 256, mic16_smem_forward(), s>>>(S, d32, r, t, S.mfaces_f, (WaveSync *)ws_f, st,
+                                                             SweepUpdate{});
     k_mic_backward16<<<S.KM, 256, mic16_smem_backward(), s>>>(S, d32, t, r, z, partials, S.mfaces_b,
                                                                (WaveSync *)ws_b, st);
     return;
@@ -1369,6 +1461,34 @@ void launch_mic_apply(const PoolSystem &S, const float *d32, const float *r, flo
   k_mic_forward<<<S.K, 64, 0, s>>>(S, S.sched, d32, r, t, faces_f, (WaveSync *)ws_f, st);
   count_launches(1);
   k_mic_backward<<<S.K, 64, 0, s>>>(S, S.sched, d32, t, r, z, partials, faces_b, (WaveSync *)ws_b, st);
+}
+
+bool launch_mic_apply_update(const PoolSystem &S, const float *d32, float *r, float *t, float *z, double *partials,
+                             const float *p, const float *q, float *x, unsigned *counter, SolverState *st,
+                             int max_iterations, void *ws_f, void *ws_b, cudaStream_t s) {
+  if (S.K <= 0 || S.KM <= 0) return false;
+  static bool attr[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64 || !attr[dev]) {
+    cudaFuncSetAttribute(k_mic_forward16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mic16_smem_forward());
+    cudaFuncSetAttribute(k_mic_backward16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mic16_smem_backward());
+    if (dev >= 0 && dev < 64) attr[dev] = true;
+  }
+  SweepUpdate fu;
+  fu.p = p;
+  fu.q = q;
+  fu.x = x;
+  fu.r = r;
+  fu.st = st;
+  fu.counter = counter;
+  fu.part = partials;  // [2 KM]; the backward sweep then writes its z.r partials over [0, KM)
+  fu.max_iterations = max_iterations;
+  count_launches(2);
+  k_mic_forward16<<<S.KM, 256, mic16_smem_forward(), s>>>(S, d32, r, t, S.mfaces_f, (WaveSync *)ws_f, st, fu);
+  k_mic_backward16<<<S.KM, 256, mic16_smem_backward(), s>>>(S, d32, t, r, z, partials, S.mfaces_b, (WaveSync *)ws_b,
+                                                             st);
+  return true;
 }
 
 void build_macro(const Geometry &G, const Geometry &M, const int *tile_count, const int *tile_state, int *macro_count,
