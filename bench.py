@@ -66,6 +66,16 @@ def job_ms_per_projection(elapsed_ms: float, steps: int, world: int, device=None
     return elapsed_ms / (steps * world)
 
 
+def measured_bf16_peak():
+    """Dense BF16 tensor peak for a kernel timed alone (burst figure)."""
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        if "bf16_tflops" in d:
+            return float(d["bf16_tflops"]), "measured"
+    return 1590.0, "fallback"
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -445,6 +455,17 @@ def main():
                        "model": os.path.relpath(model, ROOT), "steps": args.learned_steps,
                        "plain_ms_per_projection": value, "plain_iterations": last["iterations"],
                        "speedup_vs_plain": value / lms if lms else None}
+            # the network application on the tensor cores: time and FLOP rate
+            nms = ctypes.c_double()
+            ncells = ctypes.c_longlong()
+            if L.shkz_b200_time_kernel(ctx.handle, 8, 5, ctypes.byref(nms), ctypes.byref(ncells)) == 0:
+                flops = L.shkz_b200_learned_flops(ctx.handle)
+                tf = flops / (nms.value * 1e-3) / 1e12
+                bf16_peak, bf16_kind = measured_bf16_peak()
+                learned["network"] = {"ms_per_application": nms.value, "tflop_per_application": flops / 1e12,
+                                      "achieved_tflops": tf, "peak_tflops": bf16_peak, "peak_kind": bf16_kind,
+                                      "frac": tf / bf16_peak, "bound": "tensor",
+                                      "kernel": "k_conv_tc (tcgen05 implicit-GEMM 3^3 convolutions, BF16)"}
         except native.ShkzError as exc:  # reported in the line, not hidden
             learned = {"error": str(exc), "model": os.path.relpath(model, ROOT)}
         cfg.preconditioner = native.PRECOND_MIC0

@@ -200,7 +200,8 @@ int shkz_b200_apply_matrix(shkz_b200_ctx *ctx, const float *x_cells, float *y_ce
  * 256 MB write that evicts the L2, and stores the mean milliseconds per launch. which: 0 = stencil q = A p with fused p.q,
  * 1 = MIC(0) forward sweep, 2 = MIC(0) backward sweep with fused z.r,
  * 3 = fused x/r update with norms, 4 = p update, 5 = unknown labelling,
- * 6 = weights/rhs assembly, 7 = MIC(0) factor. *cells_out (may be NULL)
+ * 6 = weights/rhs assembly, 7 = MIC(0) factor, 8 = one application of the
+ * learned preconditioner's network (needs a loaded or initialised network). *cells_out (may be NULL)
  * receives the cells the kernel sweeps per launch (pool cells, or grid cells
  * for 5). No reference counterpart: it is the measurement hook for the
  * roofline figures. */
@@ -213,6 +214,10 @@ int shkz_b200_time_kernel(shkz_b200_ctx *ctx, int which, int reps, double *ms_pe
  * inspection act on the system of the last projection. */
 int shkz_b200_learned_init(shkz_b200_ctx *ctx, unsigned seed);
 long long shkz_b200_learned_param_count(shkz_b200_ctx *ctx);
+/* FLOPs of one network application on the last projection's system as the
+ * tensor cores execute it (2 * 27 * C_in * C_out per voxel of every active
+ * 8x16x8 block of each layer's level); -1 without a network. */
+double shkz_b200_learned_flops(shkz_b200_ctx *ctx);
 /* parameters blob: per layer w[27][cout][cin] then b[cout], FP32 */
 int shkz_b200_learned_set_params(shkz_b200_ctx *ctx, const float *blob, size_t n);
 int shkz_b200_learned_get_params(shkz_b200_ctx *ctx, float *blob, size_t n, int gradients);

@@ -1093,6 +1093,9 @@ extern "C" int shkz_b200_solve_csr(shkz_b200_ctx *ctx, long long n, const long l
   return rc;
 }
 
+static LearnedSystem learned_system(shkz_b200_ctx *ctx);
+static int learned_ready(shkz_b200_ctx *ctx);
+
 extern "C" int shkz_b200_time_kernel(shkz_b200_ctx *ctx, int which, int reps, double *ms, long long *cells_out) {
   if (!ctx || !ms || reps <= 0) return SHKZ_B200_ERR_ARG;
   if (!ctx->has_system) return SHKZ_B200_ERR_STATE;
@@ -1128,10 +1131,15 @@ extern "C" int shkz_b200_time_kernel(shkz_b200_ctx *ctx, int which, int reps, do
       }
       case 7: launch_mic_factor(S, ctx->colsum, ctx->cfg.mic_omega, ctx->cfg.mic_min_diag_ratio, ctx->dmic64,
                                 ctx->d32, ctx->wflags, wsync(ctx, 0), s); break;
+      case 8: learned_apply(ctx->model, learned_system(ctx), ctx->r, 1.0, ctx->t, s); break;
       default: break;
     }
   };
-  if (which < 0 || which > 7) return SHKZ_B200_ERR_ARG;
+  if (which < 0 || which > 8) return SHKZ_B200_ERR_ARG;
+  if (which == 8) {
+    const int rc = learned_ready(ctx);
+    if (rc) return rc;
+  }
   launch();  // warm-up
   SHKZ_CUDA_TRY(cudaStreamSynchronize(s));
   // Each launch is timed alone between events, after a write of a buffer
@@ -1368,6 +1376,12 @@ extern "C" int shkz_b200_learned_init(shkz_b200_ctx *ctx, unsigned seed) {
   }
   ctx->model_ready = 0;
   return learned_init_params(ctx->model, seed, ctx->stream);
+}
+
+extern "C" double shkz_b200_learned_flops(shkz_b200_ctx *ctx) {
+  if (!ctx || !ctx->model) return -1.0;
+  if (learned_ready(ctx)) return -1.0;
+  return learned_forward_flops(ctx->model);
 }
 
 extern "C" long long shkz_b200_learned_param_count(shkz_b200_ctx *ctx) {

@@ -592,6 +592,7 @@ struct LearnedModel {
   int *err = nullptr;
   double *partials = nullptr;
   size_t params_total = 0;
+  long long nactive[3] = {0, 0, 0};  // active 8x16x8 blocks per level (last prepare)
 };
 
 static size_t nvox(const LearnedModel *m, int l) { return (size_t)m->NX[l] * m->NY[l] * m->NZ[l]; }
@@ -782,6 +783,19 @@ int learned_prepare(LearnedModel *m, const Geometry &G, const int *tile_state, c
   cudaMemsetAsync(m->gpre, 0, nvox(m, 0) * 64 * 2, s);
   cudaMemsetAsync(m->gx, 0, nvox(m, 0) * 64 * 2, s);
   cudaMemsetAsync(m->err, 0, sizeof(int), s);
+  {
+    // active blocks per level, for the FLOP count of an application
+    for (int l = 0; l < 3; ++l) {
+      const size_t nb = (size_t)m->gb[l][0] * m->gb[l][1] * m->gb[l][2];
+      std::vector<uint8_t> h(nb);
+      if (cudaMemcpyAsync(h.data(), m->blk[l], nb, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+          cudaStreamSynchronize(s) != cudaSuccess)
+        return SHKZ_B200_ERR_CUDA;
+      long long c = 0;
+      for (uint8_t v : h) c += v != 0;
+      m->nactive[l] = c;
+    }
+  }
   return cudaGetLastError() == cudaSuccess ? 0 : SHKZ_B200_ERR_CUDA;
 }
 
@@ -1066,6 +1080,19 @@ int learned_output_dense(LearnedModel *m, float *Z_dense_dev, cudaStream_t s) {
 }
 
 size_t learned_dense_cells(const LearnedModel *m) { return nvox(m, 0); }
+
+// FLOPs of one application as the tensor cores execute it: every layer's 3^3
+// convolution over the active 8x16x8 blocks of its level, 2 * 27 * C_in * C_out
+// per voxel.
+double learned_forward_flops(const LearnedModel *m) {
+  double f = 0.0;
+  for (int li = 0; li < 11; ++li) {
+    const LayerDef &d = kLayers[li];
+    const double vox = (double)m->nactive[d.level] * 8 * 16 * 8;
+    f += vox * 2.0 * 27.0 * (double)(d.c0 + d.c1) * (double)d.cout;
+  }
+  return f;
+}
 
 __global__ void k_bf16_to_f32(const __nv_bfloat16 *a, size_t n, float *b) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)

@@ -26,6 +26,7 @@ int learned_get_params(LearnedModel *m, float *blob, size_t n, int grads, cudaSt
 int learned_init_params(LearnedModel *m, unsigned seed, cudaStream_t s);
 int learned_prepare(LearnedModel *m, const Geometry &G, const int *tile_state, cudaStream_t s);
 // z_pool = rmax * N(r_pool / rmax) at unknown cells
+double learned_forward_flops(const LearnedModel *m);
 int learned_apply(LearnedModel *m, const LearnedSystem &sys, const float *r_pool, double rmax, float *z_pool,
                   cudaStream_t s);
 int learned_backward_dense(LearnedModel *m, const float *gZ_dense, cudaStream_t s);

@@ -215,8 +215,14 @@ __device__ __forceinline__ void stage_tile(const PoolSystem &S, const float *__r
 
 struct Coef4 {
   float4 dg, ox, oy, oz;
+  // upper weights that no lane of this warp holds: the +x neighbour's first
+  // column (q4 == 1), the +y row (jj == 7), the +z plane (odd kk)
+  float oxf;
+  float4 oyf, ozf;
 };
 
+// All coefficient loads of a tile, issued before the tile's barrier so their
+// latency overlaps the staging of p.
 __device__ __forceinline__ Coef4 load_coef4(const PoolSystem &S, int pt) {
   const int tid = threadIdx.x;
   const int q4 = tid & 1, jj = (tid >> 1) & 7, kk = tid >> 4;
@@ -226,6 +232,25 @@ __device__ __forceinline__ Coef4 load_coef4(const PoolSystem &S, int pt) {
   c.ox = ld4(S.offx + base);
   c.oy = ld4(S.offy + base);
   c.oz = ld4(S.offz + base);
+  const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  c.oxf = 0.0f;
+  if (q4 == 1) {
+    const int nb = S.nbr[pt * 6 + NB_XP];
+    if (nb >= 0) c.oxf = S.offx[(size_t)nb * SHKZ_TC + kk * 64 + jj * 8];
+  }
+  c.oyf = zero4;
+  if (jj == 7) {
+    const int nb = S.nbr[pt * 6 + NB_YP];
+    if (nb >= 0) c.oyf = ld4(S.offy + (size_t)nb * SHKZ_TC + kk * 64 + q4 * 4);
+  }
+  c.ozf = zero4;
+  if (kk & 1) {
+    if (kk < 7) c.ozf = ld4(S.offz + base + 64);
+    else {
+      const int nb = S.nbr[pt * 6 + NB_ZP];
+      if (nb >= 0) c.ozf = ld4(S.offz + (size_t)nb * SHKZ_TC + jj * 8 + q4 * 4);
+    }
+  }
   return c;
 }
 
@@ -246,25 +271,9 @@ __device__ __forceinline__ float4 stencil4(const PoolSystem &S, int pt, const Sp
   ozn.y = __shfl_down_sync(0xffffffffu, oz.y, 16);
   ozn.z = __shfl_down_sync(0xffffffffu, oz.z, 16);
   ozn.w = __shfl_down_sync(0xffffffffu, oz.w, 16);
-  float oxu3;
-  if (q4 == 0) oxu3 = oxn;
-  else {
-    const int nb = S.nbr[pt * 6 + NB_XP];
-    oxu3 = nb >= 0 ? S.offx[(size_t)nb * SHKZ_TC + kk * 64 + jj * 8] : 0.0f;
-  }
-  float4 oyu;
-  if (jj < 7) oyu = oyn;
-  else {
-    const int nb = S.nbr[pt * 6 + NB_YP];
-    oyu = nb >= 0 ? ld4(S.offy + (size_t)nb * SHKZ_TC + kk * 64 + q4 * 4) : make_float4(0.f, 0.f, 0.f, 0.f);
-  }
-  float4 ozu;
-  if ((kk & 1) == 0) ozu = ozn;
-  else if (kk < 7) ozu = ld4(S.offz + base + 64);
-  else {
-    const int nb = S.nbr[pt * 6 + NB_ZP];
-    ozu = nb >= 0 ? ld4(S.offz + (size_t)nb * SHKZ_TC + jj * 8 + q4 * 4) : make_float4(0.f, 0.f, 0.f, 0.f);
-  }
+  const float oxu3 = q4 == 0 ? oxn : cf.oxf;
+  const float4 oyu = jj < 7 ? oyn : cf.oyf;
+  const float4 ozu = (kk & 1) == 0 ? ozn : cf.ozf;
   const float oxu[4] = {ox.y, ox.z, ox.w, oxu3};
   float out[4];
   #pragma unroll
@@ -287,7 +296,8 @@ __device__ __forceinline__ float4 stencil4(const PoolSystem &S, int pt, const Sp
 
 // mode 0: q = A p and pq = p.q -> st->pq, st->alpha = rho/pq
 // mode 1: q = A p only
-__global__ void __launch_bounds__(128, 10) k_spmv(PoolSystem S, const float *__restrict__ p, float *__restrict__ q,
+#define SPMV_CTAS_PER_SM 8
+__global__ void __launch_bounds__(128, SPMV_CTAS_PER_SM) k_spmv(PoolSystem S, const float *__restrict__ p, float *__restrict__ q,
                                               double *partials, unsigned *counter, SolverState *st, int mode) {
   __shared__ SpmvSmem sm;
   __shared__ double red[4];
@@ -1403,7 +1413,8 @@ void launch_spmv(const PoolSystem &S, const float *p, float *q, double *partials
   k_spmv<<<spmv_grid(S.K), 128, 0, s>>>(S, p, q, partials, counter, st, mode);
 }
 
-int spmv_grid(int K) { return K < 148 * 12 ? K : 148 * 12; }
+// one wave of resident CTAs looping over the tiles
+int spmv_grid(int K) { return K < 148 * SPMV_CTAS_PER_SM ? K : 148 * SPMV_CTAS_PER_SM; }
 
 void launch_update_xr(int n, const float *p, const float *q, float *x, float *r, double *partials, unsigned *counter,
                       SolverState *st, int max_iterations, cudaStream_t s) {

@@ -88,6 +88,7 @@ EXPORTS = [
     "shkz_b200_learned_save", "shkz_b200_learned_load", "shkz_b200_conv3d", "shkz_b200_conv3d_noalloc",
     "shkz_b200_set_target_volume", "shkz_b200_get_volume_state", "shkz_b200_set_volume_state",
     "shkz_b200_warm_start_size", "shkz_b200_get_warm_start", "shkz_b200_set_warm_start",
+    "shkz_b200_learned_flops",
 ]
 
 _lib = None
@@ -120,6 +121,8 @@ def load(path: str = LIB_PATH):
     L.shkz_b200_set_target_volume.argtypes = [P, ctypes.c_double, ctypes.c_double]
     L.shkz_b200_get_volume_state.argtypes = [P, P]
     L.shkz_b200_set_volume_state.argtypes = [P, P]
+    L.shkz_b200_learned_flops.argtypes = [P]
+    L.shkz_b200_learned_flops.restype = ctypes.c_double
     L.shkz_b200_warm_start_size.argtypes = [P]
     L.shkz_b200_warm_start_size.restype = ctypes.c_longlong
     L.shkz_b200_get_warm_start.argtypes = [P, P, ctypes.c_size_t]
