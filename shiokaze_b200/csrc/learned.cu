@@ -78,32 +78,41 @@ __global__ void __launch_bounds__(128, 1) k_conv_tc(ConvArgs a) {
   const int nchunk = (a.c0 + a.c1) / 16;
   const uint32_t idesc = umma_idesc_bf16(a.cout);
   const uint32_t halo_s = smem_u32(halo), w_s = smem_u32(wsm), bar_s = smem_u32(mbar);
-  const int per_k = (P + 2) * 180;
   bool ok = true;
   for (int ch = 0; ch < nchunk; ++ch) {
-    for (int e = tid; e < 2 * per_k; e += 128) {
-      const int kh = e / per_k;
-      int r = e - kh * per_k;
-      const int zz = r / 180;
-      r -= zz * 180;
-      const int yy = r / 10, xx = r - yy * 10;
-      const int X = X0 + xx - 1, Y = Y0 + yy - 1, Z = Z0 + zz - 1;
-      const int c = ch * 16 + kh * 8;
-      const void *src = a.in0;
-      int bytes = 0;
-      if (X >= 0 && Y >= 0 && Z >= 0 && X < a.nx && Y < a.ny && Z < a.nz) {
-        if (c < a.c0) {
-          src = a.in0 + ((size_t)((size_t)Z * a.ny + Y) * a.nx + X) * a.c0 + c;
-          bytes = 16;
+    // halo of the chunk: each thread owns one or two of the 18 x 10 (y, x)
+    // columns and walks its P + 2 planes and both 8-channel halves, so the
+    // index arithmetic is done once per column, not per 16-byte copy
+    const bool first = ch * 16 < a.c0;  // chunk from in0 (else the upsampled in1)
+    for (int pp = tid; pp < 180; pp += 128) {
+      const int yy = pp / 10, xx = pp - yy * 10;
+      const int X = X0 + xx - 1, Y = Y0 + yy - 1;
+      const bool inxy = X >= 0 && Y >= 0 && X < a.nx && Y < a.ny;
+      const int hX = X >> 1, hY = Y >> 1;
+      const bool inxy1 = inxy && hX < a.hx && hY < a.hy;
+      const uint32_t dcol = halo_s + (uint32_t)(yy * 10 + xx) * 16;
+      for (int zz = 0; zz < P + 2; ++zz) {
+        const int Z = Z0 + zz - 1;
+        const void *src0 = a.in0, *src1 = a.in0;
+        int bytes = 0;
+        if (first) {
+          if (inxy && Z >= 0 && Z < a.nz) {
+            src0 = a.in0 + ((size_t)((size_t)Z * a.ny + Y) * a.nx + X) * a.c0 + ch * 16;
+            src1 = static_cast<const __nv_bfloat16 *>(src0) + 8;
+            bytes = 16;
+          }
         } else {
-          const int hX = X >> 1, hY = Y >> 1, hZ = Z >> 1;
-          if (hX < a.hx && hY < a.hy && hZ < a.hz) {
-            src = a.in1 + ((size_t)((size_t)hZ * a.hy + hY) * a.hx + hX) * a.c1 + (c - a.c0);
+          const int hZ = Z >> 1;
+          if (inxy1 && Z >= 0 && Z < a.nz && hZ < a.hz) {
+            src0 = a.in1 + ((size_t)((size_t)hZ * a.hy + hY) * a.hx + hX) * a.c1 + (ch * 16 - a.c0);
+            src1 = static_cast<const __nv_bfloat16 *>(src0) + 8;
             bytes = 16;
           }
         }
+        const uint32_t d = dcol + (uint32_t)zz * 180 * 16;
+        cp_async16(d, src0, bytes);
+        cp_async16(d + LBO_A, src1, bytes);
       }
-      cp_async16(halo_s + kh * LBO_A + ((zz * 18 + yy) * 10 + xx) * 16, src, bytes);
     }
     const __nv_bfloat16 *wsrc = a.wpk + (size_t)ch * 27 * a.cout * 16;
     for (int e = tid; e < 27 * a.cout * 2; e += 128) cp_async16(w_s + e * 16, wsrc + (size_t)e * 8, 16);
