@@ -24,6 +24,8 @@
  * calls the C ABI (include/shkz_b200.h); all arithmetic runs on the GPU.
  * Errors never throw: a failed solve is reported on the console and the
  * record, and the velocity is left unprojected with 0 iterations recorded.
+ * With B200.Strict=Yes a failure ends the program instead (exit status 1),
+ * as the reference's loader does on fatal errors (src/core/module.cpp:141).
  */
 #include <shiokaze/array/array3.h>
 #include <shiokaze/array/macarray3.h>
@@ -33,6 +35,7 @@
 #include <shiokaze/core/timer.h>
 #include "shkz_b200.h"
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 //
@@ -82,6 +85,7 @@ protected:
 			if( rc ) {
 				console::dump( "shkz_b200_create failed: %s\n", shkz_b200_errstr(rc));
 				console::write(get_argument_name()+"_number_projection_iteration", 0);
+				if( m_strict ) std::exit(1);
 				return;
 			}
 			if( m_prev_pending ) {
@@ -136,6 +140,7 @@ protected:
 		console::write(get_argument_name()+"_reresid_l2", res.reresid_l2);
 		if( rc ) {
 			console::dump( "failed: %s (%s)\n", shkz_b200_errstr(rc), shkz_b200_last_error(m_ctx));
+			if( m_strict ) std::exit(1);
 			return;
 		}
 		console::dump( "Done. Took %d iterations, Reresid=%e. Took %s\n", res.iterations, res.reresid, timer.stock("linsolve").c_str());
@@ -192,6 +197,7 @@ protected:
 		int device = m_cfg.device;
 		config.get_integer("B200.Device",device,"CUDA device ordinal");
 		m_cfg.device = device;
+		config.get_bool("B200.Strict",m_strict,"End the program when the GPU projection fails");
 		m_cfg.second_order_fluid = m_param.second_order_accurate_fluid;
 		m_cfg.second_order_solid = m_param.second_order_accurate_solid;
 	}
@@ -258,6 +264,7 @@ protected:
 		return c;
 	}
 	shkz_b200_ctx *m_ctx {nullptr};
+	bool m_strict {false};
 	//
 	shape3 m_shape;
 	double m_dx {0.0};

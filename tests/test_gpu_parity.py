@@ -266,3 +266,39 @@ def test_solve_csr_matches_shipped_pcg(golden):
     # two FP64 CG runs with different summation orders stop at the same count
     # but hold different iterates; the bar of the shipped mode applies
     assert rel_inf(p, g["pressure_shipped"]) <= max(PARITY_TOL, 10 * float(g["tol"]))
+
+
+def test_tile_activity_matches_reference(golden):
+    """Tile activity: the pool holds exactly the 8^3 tiles in which the
+    reference's pressure grid has an active cell (its allocated tiles)."""
+    name, g = golden
+    sc = GoldenScene(g)
+    s, res, _ = run(sc, Residual=float(g["tol"]))
+    act = g["pressure_active"].astype(bool)
+    nz, ny, nx = act.shape
+    pad = np.zeros(((nz + 7) // 8 * 8, (ny + 7) // 8 * 8, (nx + 7) // 8 * 8), bool)
+    pad[:nz, :ny, :nx] = act
+    tiles = pad.reshape(pad.shape[0] // 8, 8, pad.shape[1] // 8, 8, pad.shape[2] // 8, 8).any(axis=(1, 3, 5))
+    assert res["tiles"] == int(tiles.sum())
+    assert res["unknowns"] == int(act.sum())
+
+
+def test_size_limits_are_errors_not_faults():
+    """Grids beyond the documented limits are refused before any device work."""
+    import ctypes
+    from shiokaze_b200 import native
+    ctx = native.Context(native.default_config())
+    a = native.ProjectArgs()
+    a.nx, a.ny, a.nz, a.dx, a.dt = 70000, 8, 8, 1.0, 1.0
+    buf = np.zeros(8, np.float32)
+    m = np.zeros(8, np.uint8)
+    a.fluid, a.fluid_active = buf.ctypes.data, m.ctypes.data
+    for d in range(3):
+        a.velocity[d] = buf.ctypes.data
+        a.velocity_active[d] = m.ctypes.data
+    res = native.Result()
+    rc = native.load().shkz_b200_project_device(ctx.handle, ctypes.byref(a), ctypes.byref(res))
+    assert rc == -8  # SHKZ_B200_ERR_LIMIT
+    a.nx = 0
+    rc = native.load().shkz_b200_project_device(ctx.handle, ctypes.byref(a), ctypes.byref(res))
+    assert rc == -1  # SHKZ_B200_ERR_ARG
