@@ -121,20 +121,26 @@ __global__ void __launch_bounds__(128, 1) k_conv_tc(ConvArgs a) {
     __syncthreads();
     if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      // The descriptors' start-address field holds (address >> 4) in its low
+      // 14 bits and shared addresses stay below 2^18, so a tap's descriptor is
+      // the base descriptor plus the tap's offset in 16-byte units.
+      const uint64_t da0 = umma_desc(halo_s, LBO_A, 160);
+      const uint64_t db0 = umma_desc(w_s, (uint32_t)a.cout * 16, 128);
       for (int zo = 0; zo < P; ++zo) {
-        for (int t = 0; t < 27; ++t) {
-          const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
-          const uint32_t a_addr = halo_s + (uint32_t)(((zo + dz) * 18 + dy) * 10 + dx) * 16;
-          const uint64_t da = umma_desc(a_addr, LBO_A, 160);
-          const uint64_t db = umma_desc(w_s + (uint32_t)t * a.cout * 32, (uint32_t)a.cout * 16, 128);
-          const uint32_t d_tmem = tmem + (uint32_t)(zo * pstride);
-          const uint32_t acc = (ch > 0 || t > 0) ? 1u : 0u;
-          asm volatile(
-              "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-              "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(d_tmem),
-              "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0)
-              : "memory");
-        }
+        const uint32_t d_tmem = tmem + (uint32_t)(zo * pstride);
+        int t = 0;
+        for (int dz = 0; dz < 3; ++dz)
+          for (int dy = 0; dy < 3; ++dy)
+            for (int dx = 0; dx < 3; ++dx, ++t) {
+              const uint64_t da = da0 + (uint64_t)(((zo + dz) * 18 + dy) * 10 + dx);
+              const uint64_t db = db0 + (uint64_t)(t * a.cout * 2);
+              const uint32_t acc = (ch > 0 || t > 0) ? 1u : 0u;
+              asm volatile(
+                  "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                  "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(d_tmem),
+                  "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0)
+                  : "memory");
+            }
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar_s)
                    : "memory");
