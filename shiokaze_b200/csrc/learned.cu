@@ -23,6 +23,8 @@
 #include "solver.h"
 #include "tc_conv.cuh"
 
+#include <cudaTypedefs.h>
+
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -34,7 +36,7 @@ namespace shkz {
 // ---------------------------------------------------------------------------
 // tcgen05 convolution kernel
 
-__global__ void __launch_bounds__(128, 1) k_conv_tc(ConvArgs a) {
+__global__ void __launch_bounds__(128, 1) k_conv_tc(ConvArgs a, const __grid_constant__ ConvMaps maps) {
   extern __shared__ __align__(1024) uint8_t smem[];
   const int P = a.planes;
   const uint32_t LBO_A = (uint32_t)(P + 2) * 18 * 10 * 16;
@@ -42,7 +44,8 @@ __global__ void __launch_bounds__(128, 1) k_conv_tc(ConvArgs a) {
   uint8_t *halo = smem;
   uint8_t *wsm = smem + 2 * LBO_A;
   uint64_t *mbar = reinterpret_cast<uint64_t *>(wsm + wbytes);
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mbar + 1);
+  uint64_t *mbar_tma = mbar + 1;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mbar + 2);
 
   const int zsplit = 8 / P;
   int bid = blockIdx.x;
@@ -68,6 +71,7 @@ __global__ void __launch_bounds__(128, 1) k_conv_tc(ConvArgs a) {
   }
   if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar)) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar_tma)) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -79,12 +83,32 @@ __global__ void __launch_bounds__(128, 1) k_conv_tc(ConvArgs a) {
   const uint32_t idesc = umma_idesc_bf16(a.cout);
   const uint32_t halo_s = smem_u32(halo), w_s = smem_u32(wsm), bar_s = smem_u32(mbar);
   bool ok = true;
+  const uint32_t tma_s = smem_u32(mbar_tma);
+  int tma_uses = 0;
   for (int ch = 0; ch < nchunk; ++ch) {
-    // halo of the chunk: each thread owns one or two of the 18 x 10 (y, x)
-    // columns and walks its P + 2 planes and both 8-channel halves, so the
-    // index arithmetic is done once per column, not per 16-byte copy
     const bool first = ch * 16 < a.c0;  // chunk from in0 (else the upsampled in1)
-    for (int pp = tid; pp < 180; pp += 128) {
+    const bool by_tma = a.tma && first;
+    if (by_tma) {
+      // both 8-channel halves of the halo by two 4D TMA loads; the tensor maps
+      // cover the grid exactly, so halo voxels outside it arrive as zeros
+      if (tid == 0) {
+        const uint32_t bytes = 2 * LBO_A;
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tma_s), "r"(bytes) : "memory");
+        #pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const CUtensorMap *map = &maps.m[2 * ch + h];
+          asm volatile(
+              "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];" ::
+                  "r"(halo_s + (uint32_t)h * LBO_A), "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(X0 - 1),
+                  "r"(Y0 - 1), "r"(Z0 - 1), "r"(tma_s)
+              : "memory");
+        }
+      }
+    }
+    // halo of the chunk (unless by TMA): each thread owns one or two of the
+    // 18 x 10 (y, x) columns and walks its P + 2 planes and both 8-channel
+    // halves, so the index arithmetic is done once per column
+    for (int pp = by_tma ? 180 : tid; pp < 180; pp += 128) {
       const int yy = pp / 10, xx = pp - yy * 10;
       const int X = X0 + xx - 1, Y = Y0 + yy - 1;
       const bool inxy = X >= 0 && Y >= 0 && X < a.nx && Y < a.ny;
@@ -117,8 +141,13 @@ __global__ void __launch_bounds__(128, 1) k_conv_tc(ConvArgs a) {
     const __nv_bfloat16 *wsrc = a.wpk + (size_t)ch * 27 * a.cout * 16;
     for (int e = tid; e < 27 * a.cout * 2; e += 128) cp_async16(w_s + e * 16, wsrc + (size_t)e * 8, 16);
     cp_async_wait_all();
+    if (by_tma) {
+      if (mbar_wait(tma_s, (uint32_t)(tma_uses & 1))) ++tma_uses;
+      else ok = false;  // tma_uses keeps the parity still in flight for the error path
+    }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
+    if (!ok) break;
     if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       // The descriptors' start-address field holds (address >> 4) in its low
@@ -189,9 +218,11 @@ __global__ void __launch_bounds__(128, 1) k_conv_tc(ConvArgs a) {
     }
   } else {
     if (tid == 0) atomicExch(a.err, 1);
-    // give the outstanding MMAs a bounded chance to finish before TMEM is freed
+    // give the outstanding MMAs and halo copies a bounded chance to finish
+    // before TMEM and shared memory are released
     mbar_wait(bar_s, 0);
     mbar_wait(bar_s, 1);
+    if (a.tma) mbar_wait(tma_s, (uint32_t)(tma_uses & 1));
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
@@ -200,7 +231,55 @@ __global__ void __launch_bounds__(128, 1) k_conv_tc(ConvArgs a) {
 }
 
 static size_t conv_smem_bytes(int planes, int cout) {
-  return (size_t)2 * (planes + 2) * 18 * 10 * 16 + (size_t)27 * cout * 32 + 16;
+  return (size_t)2 * (planes + 2) * 18 * 10 * 16 + (size_t)27 * cout * 32 + 32;
+}
+
+// cuTensorMapEncodeTiled from the driver, looked up once.
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+// Tensor maps for the in0 chunks of a convolution; false (a.tma stays 0, all
+// halos by cp.async) when the driver entry point is missing, the channel
+// count exceeds the maps' capacity or the driver rejects a map.
+static bool make_conv_maps(ConvArgs &a, ConvMaps &M) {
+  a.tma = 0;
+  auto enc = tensor_map_encoder();
+  const int nch0 = a.c0 / 16;
+  if (!enc || nch0 > CONV_MAX_TMA_CHUNKS || a.c0 % 16) return false;
+  for (int ch = 0; ch < nch0; ++ch)
+    for (int h = 0; h < 2; ++h) {
+      const __nv_bfloat16 *base = a.in0 + ch * 16 + h * 8;  // 16-byte aligned: 32 ch + 16 h bytes past the tensor
+      const cuuint64_t dims[4] = {8, (cuuint64_t)a.nx, (cuuint64_t)a.ny, (cuuint64_t)a.nz};
+      const cuuint64_t strides[3] = {(cuuint64_t)a.c0 * 2, (cuuint64_t)a.nx * a.c0 * 2,
+                                     (cuuint64_t)a.ny * a.nx * a.c0 * 2};
+      const cuuint32_t box[4] = {8, 10, 18, (cuuint32_t)(a.planes + 2)};
+      const cuuint32_t es[4] = {1, 1, 1, 1};
+      if (enc(&M.m[2 * ch + h], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16 *>(base), dims, strides,
+              box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
+    }
+  a.tma = 1;
+  return true;
+}
+
+static void launch_conv_tc(ConvArgs a, int nblocks, size_t smem, cudaStream_t s) {
+  ConvMaps maps;  // the launch copies it into the kernel's parameter buffer
+  std::memset(&maps, 0, sizeof(maps));
+  make_conv_maps(a, maps);
+  count_launches(1);
+  k_conv_tc<<<nblocks, 128, smem, s>>>(a, maps);
 }
 
 // ---------------------------------------------------------------------------
@@ -844,8 +923,7 @@ static int conv_launch(LearnedModel *m, int level, const __nv_bfloat16 *in0, int
   const size_t smem = conv_smem_bytes(a.planes, cout);
   cudaFuncSetAttribute(k_conv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   const int nblocks = a.gbx * a.gby * a.gbz * (8 / a.planes);
-  count_launches(1);
-  k_conv_tc<<<nblocks, 128, smem, s>>>(a);
+  launch_conv_tc(a, nblocks, smem, s);
   return cudaGetLastError() == cudaSuccess ? 0 : SHKZ_B200_ERR_CUDA;
 }
 
@@ -987,7 +1065,7 @@ int conv3d_run(int nx, int ny, int nz, int c0, int c1, int cout, int planes, con
     cudaMemset(act, 1, (size_t)gbx * gby * gbz);
     cudaMemset(err, 0, 4);
     cudaMemset(dout, 0, n0 * n_pad * 2);
-    count_launches(2);
+    count_launches(1);
     k_pack_weights<<<256, 256>>>(dwf, cout, cin, n_pad, cin, 0, dw);
     ConvArgs a;
     a.in0 = d0;
@@ -1008,7 +1086,7 @@ int conv3d_run(int nx, int ny, int nz, int c0, int c1, int cout, int planes, con
     a.planes = planes;
     a.err = err;
     cudaFuncSetAttribute(k_conv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    k_conv_tc<<<gbx * gby * gbz * (8 / planes), 128, conv_smem_bytes(planes, n_pad)>>>(a);
+    launch_conv_tc(a, gbx * gby * gbz * (8 / planes), conv_smem_bytes(planes, n_pad), 0);
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) rc = SHKZ_B200_ERR_CUDA;
     int herr = 0;
@@ -1038,7 +1116,7 @@ int conv3d_launch_scratch(int nx, int ny, int nz, int c0, int c1, int cout, int 
   const int cin = c0 + c1;
   const int gbx = (nx + 7) / 8, gby = (ny + 15) / 16, gbz = (nz + 7) / 8;
   const int nb = gbx * gby * gbz;
-  count_launches(3);
+  count_launches(2);
   k_pack_weights<<<256, 256, 0, s>>>(w, cout, cin, cout, cin, 0, wpk);
   k_fill_u8<<<grid_blocks((size_t)nb, 256, 1024), 256, 0, s>>>(act, nb, 1);
   if (cudaMemsetAsync(err, 0, sizeof(int), s) != cudaSuccess) return SHKZ_B200_ERR_CUDA;
@@ -1062,7 +1140,7 @@ int conv3d_launch_scratch(int nx, int ny, int nz, int c0, int c1, int cout, int 
   a.err = err;
   if (cudaFuncSetAttribute(k_conv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess)
     return SHKZ_B200_ERR_CUDA;
-  k_conv_tc<<<nb * (8 / planes), 128, conv_smem_bytes(planes, cout), s>>>(a);
+  launch_conv_tc(a, nb * (8 / planes), conv_smem_bytes(planes, cout), s);
   return cudaGetLastError() == cudaSuccess ? 0 : SHKZ_B200_ERR_CUDA;
 }
 

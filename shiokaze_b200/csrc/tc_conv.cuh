@@ -21,6 +21,7 @@
 // The epilogue reads each warp's 32 TMEM lanes (rows) with tcgen05.ld, adds
 // the bias, applies ReLU and stores BF16 channels-last (or channel 0 in FP32).
 #pragma once
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <stdint.h>
 
@@ -43,6 +44,16 @@ struct ConvArgs {
   int gbx, gby, gbz;          // blocks per axis
   int planes;                 // 8 or 4 z planes per CTA
   int *err;                   // set on a bounded-wait timeout
+  int tma;                    // 1: in0 halos by TMA through the tensor maps of ConvMaps
+};
+
+// Tensor maps of the in0 halos: chunk ch, 8-channel half h at m[2 ch + h],
+// each a 4D view (8 channels, x, y, z) of the channels-last tensor starting at
+// channel 16 ch + 8 h, box (8, 10, 18, P + 2), no swizzle, zero fill outside
+// the grid. Passed as a __grid_constant__ kernel parameter.
+#define CONV_MAX_TMA_CHUNKS 8
+struct ConvMaps {
+  CUtensorMap m[2 * CONV_MAX_TMA_CHUNKS];
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
