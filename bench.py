@@ -226,8 +226,9 @@ def main():
     ap.add_argument("--mic-block", type=int, default=16, choices=[8, 16],
                     help="MIC(0) sweep block edge (16: 2x2x2 tiles per CTA)")
     ap.add_argument("--model", default=None, help="trained network for the learned preconditioner")
-    ap.add_argument("--scene", default="sloshing_tank", choices=["sloshing_tank", "splash", "dambreak_rain"],
-                    help="sloshing_tank 256^3 (headline), splash 384^3, dambreak_rain 512^3")
+    ap.add_argument("--scene", default="sloshing_tank",
+                    choices=["sloshing_tank", "splash", "dambreak_rain", "dambreak_sphere"],
+                    help="sloshing_tank 256^3 (headline), splash 384^3, dambreak_rain 512^3, dambreak_sphere 64^3")
     ap.add_argument("--learned-steps", type=int, default=2,
                     help="timed projections of the learned-preconditioner arm (0: skip)")
     args = ap.parse_args()
@@ -252,12 +253,15 @@ def main():
         sc = scenes.sloshing_tank(n=args.n, seed=0, tol=1e-6)
     elif args.scene == "splash":
         sc = scenes.splash(n=args.n if args.n != 256 else 384, seed=0, tol=1e-6)
-    else:
+    elif args.scene == "dambreak_rain":
         sc = scenes.dambreak_rain(n=args.n if args.n != 256 else 512, seed=0, tol=1e-6)
+    else:
+        # the CPU-runnable configuration: 64^3 dam break + sphere, tolerance 1e-4
+        sc = scenes.dambreak_sphere(n=args.n if args.n != 256 else 64, seed=0)
     nx, ny, nz = sc.nx, sc.ny, sc.nz
 
     cfg = native.default_config()
-    cfg.residual = 1e-6
+    cfg.residual = sc.tol
     cfg.preconditioner = {"mic0": native.PRECOND_MIC0, "none": native.PRECOND_NONE,
                           "learned": native.PRECOND_LEARNED}[args.precond]
     cfg.device = local
@@ -484,7 +488,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": value, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 (f64 reductions, refinement and assembly)", "data": "synthetic",
             "config": {"workload": f"{args.scene} {nx}^3, {'plain MIC(0)' if args.precond == 'mic0' else args.precond}"
-                                   f"-PCG projection to 1e-6 (inf-norm), FP64 refinement, seed 0",
+                                   f"-PCG projection to {sc.tol:g} (inf-norm), FP64 refinement, seed 0",
                        "preconditioner": args.precond,
                        "unknowns": last["unknowns"], "pool_tiles": last["tiles"],
                        "l2": "inputs (0.42 GB at 256^3) and pool arrays > 126 MB L2 (no flush needed)",
