@@ -767,6 +767,16 @@ __global__ void __launch_bounds__(64) k_mic_backward(PoolSystem S, const int *sc
 
 #define MT 16
 #define MTC 4096
+// Solution array of a macro tile with one ghost layer: cell (x, y, z),
+// x, y, z in [-1, 16], at (x + 1) + 18 (y + 1) + 337 (z + 1). The ghosts hold
+// the upstream faces, so the sweep's neighbour reads are unconditional. Along
+// a diagonal (x = s - y - z) consecutive rows are 17 floats apart and the
+// warp's second plane 336 = 16 (mod 32) further, so its 32 rows fall in 32
+// distinct banks.
+#define MGY 18
+#define MGZ 337
+#define MGC 6080            // >= 18 * 337, padded to 16 bytes
+__device__ __forceinline__ int mghost(int x, int y, int z) { return (x + 1) + MGY * (y + 1) + MGZ * (z + 1); }
 
 // macro tile counts = sum of the counts of its (up to) eight tiles
 __global__ void k_macro_count(Geometry G, const int *tile_count, Geometry M, int *macro_count) {
@@ -862,6 +872,19 @@ __device__ __forceinline__ void macro_load_update(const int *sub, float *r, cons
   }
 }
 
+// Write the interior of a ghosted solution array back to the pool sub-tiles.
+__device__ __forceinline__ void macro_store_ghosted(const int *sub, const float *srcg, float *dst) {
+  for (int e = threadIdx.x; e < 8 * 128; e += blockDim.x) {
+    const int v = e & 127, st = e >> 7;
+    const int pt = sub[st];
+    if (pt < 0) continue;
+    const int c = v * 4;
+    const int x = (c & 7) + (st & 1) * 8, y = ((c >> 3) & 7) + ((st >> 1) & 1) * 8, z = (c >> 6) + (st >> 2) * 8;
+    const int o = mghost(x, y, z);
+    reinterpret_cast<float4 *>(dst + (size_t)pt * SHKZ_TC)[v] = make_float4(srcg[o], srcg[o + 1], srcg[o + 2], srcg[o + 3]);
+  }
+}
+
 __device__ __forceinline__ void macro_store(const int *sub, const float *srcs, float *dst) {
   for (int e = threadIdx.x; e < 8 * 128; e += blockDim.x) {
     const int v = e & 127, st = e >> 7;
@@ -891,8 +914,7 @@ __global__ void __launch_bounds__(256) k_mic_forward16(PoolSystem S, const float
                                                        unsigned long long *faces, WaveSync *ws, const SolverState *st,
                                                        SweepUpdate fu) {
   extern __shared__ __align__(16) float smf[];
-  float *T = smf, *R = T + MTC, *Dd = R + MTC, *WX = Dd + MTC, *WY = WX + MTC, *WZ = WY + MTC;
-  float *hx = WZ + MTC, *hy = hx + 256, *hz = hy + 256;
+  float *Tg = smf, *R = Tg + MGC, *Dd = R + MTC, *WX = Dd + MTC, *WY = WX + MTC, *WZ = WY + MTC;
   __shared__ int sub[8];
   if (st && st->done) return;
   int slot, epoch;
@@ -916,33 +938,37 @@ __global__ void __launch_bounds__(256) k_mic_forward16(PoolSystem S, const float
     macro_load5(sub, r, d32, S.offx, S.offy, S.offz, R, Dd, WX, WY, WZ);
   }
   {
+    // upstream faces straight into the ghost layer (x = -1, y = -1, z = -1)
     const int nxm = S.mnbr[mt * 6 + NB_XM], nym = S.mnbr[mt * 6 + NB_YM], nzm = S.mnbr[mt * 6 + NB_ZM];
+    const int u = tid & 15, v = tid >> 4;
     bool ok = true;
-    hx[tid] = nxm >= 0 ? face_get(faces + ((size_t)nxm * 3 + 0) * 256 + tid, epoch, ok) : 0.0f;
-    hy[tid] = nym >= 0 ? face_get(faces + ((size_t)nym * 3 + 1) * 256 + tid, epoch, ok) : 0.0f;
-    hz[tid] = nzm >= 0 ? face_get(faces + ((size_t)nzm * 3 + 2) * 256 + tid, epoch, ok) : 0.0f;
+    Tg[mghost(-1, u, v)] = nxm >= 0 ? face_get(faces + ((size_t)nxm * 3 + 0) * 256 + tid, epoch, ok) : 0.0f;
+    Tg[mghost(u, -1, v)] = nym >= 0 ? face_get(faces + ((size_t)nym * 3 + 1) * 256 + tid, epoch, ok) : 0.0f;
+    Tg[mghost(u, v, -1)] = nzm >= 0 ? face_get(faces + ((size_t)nzm * 3 + 2) * 256 + tid, epoch, ok) : 0.0f;
     if (!ok) atomicCAS(&ws->error, 0, slot + 1);
   }
   __syncthreads();
-  for (int s = 0; s < 3 * MT - 2; ++s) {
-    const int ii = s - jj - kk;
-    if (ii >= 0 && ii < MT) {
-      const int c = ii + MT * jj + MT * MT * kk;
-      const float tx = ii > 0 ? T[c - 1] : hx[jj + MT * kk];
-      const float ty = jj > 0 ? T[c - MT] : hy[ii + MT * kk];
-      const float tz = kk > 0 ? T[c - MT * MT] : hz[ii + MT * jj];
-      T[c] = Dd[c] * (R[c] + WX[c] * tx + WY[c] * ty + WZ[c] * tz);
+  {
+    // cell ii = s - jj - kk of the thread's row: coefficient index s + cb,
+    // ghosted index s + gb; neighbour reads need no boundary test
+    const int cb = 15 * jj + 255 * kk, gb = mghost(0, jj, kk) - jj - kk;
+    for (int s = 0; s < 3 * MT - 2; ++s) {
+      if ((unsigned)(s - jj - kk) < (unsigned)MT) {
+        const int c = s + cb, g = s + gb;
+        const float tx = Tg[g - 1], ty = Tg[g - MGY], tz = Tg[g - MGZ];
+        Tg[g] = Dd[c] * (R[c] + WX[c] * tx + WY[c] * ty + WZ[c] * tz);
+      }
+      __syncthreads();
     }
-    __syncthreads();
   }
   {
     unsigned long long *f = faces + (size_t)mt * 3 * 256;
     const int u = tid & 15, v = tid >> 4;
-    face_put(f + 0 * 256 + tid, epoch, T[15 + MT * u + MT * MT * v]);
-    face_put(f + 1 * 256 + tid, epoch, T[u + MT * 15 + MT * MT * v]);
-    face_put(f + 2 * 256 + tid, epoch, T[u + MT * v + MT * MT * 15]);
+    face_put(f + 0 * 256 + tid, epoch, Tg[mghost(15, u, v)]);
+    face_put(f + 1 * 256 + tid, epoch, Tg[mghost(u, 15, v)]);
+    face_put(f + 2 * 256 + tid, epoch, Tg[mghost(u, v, 15)]);
   }
-  macro_store(sub, T, t);
+  macro_store_ghosted(sub, Tg, t);
   if (fu.st && last_block(fu.counter)) {
     // the convergence bookkeeping of k_update_xr, on the new residual
     __shared__ double red2[8];
@@ -975,8 +1001,7 @@ __global__ void __launch_bounds__(256) k_mic_backward16(PoolSystem S, const floa
                                                         unsigned long long *faces, WaveSync *ws,
                                                         const SolverState *st) {
   extern __shared__ __align__(16) float smb[];
-  float *Z = smb, *Tt = Z + MTC, *Dd = Tt + MTC, *WX = Dd + MTC, *WY = WX + MTC, *WZ = WY + MTC;
-  float *hx = WZ + MTC, *hy = hx + 256, *hz = hy + 256, *ux = hz + 256, *uy = ux + 256, *uz = uy + 256;
+  float *Zg = smb, *Tt = Zg + MGC, *Dd = Tt + MTC, *WX = Dd + MTC, *WY = WX + MTC, *WZ = WY + MTC;
   __shared__ int sub[8];
   __shared__ double red[8];
   if (st && st->done) return;
@@ -988,11 +1013,11 @@ __global__ void __launch_bounds__(256) k_mic_backward16(PoolSystem S, const floa
   __syncthreads();
   macro_load5(sub, t, d32, S.offx, S.offy, S.offz, Tt, Dd, WX, WY, WZ);
   const int nxp = S.mnbr[mt * 6 + NB_XP], nyp = S.mnbr[mt * 6 + NB_YP], nzp = S.mnbr[mt * 6 + NB_ZP];
+  float wxv = 0.f, wyv = 0.f, wzv = 0.f;
   {
     // upper weights across the macro faces: lower weights of the +x/+y/+z
     // macro neighbours' first column/row/plane, from their pool sub-tiles
     const int u = tid & 15, v = tid >> 4;
-    float wxv = 0.f, wyv = 0.f, wzv = 0.f;
     if (nxp >= 0) {  // cell (0, u, v) of the +x macro tile
       const int pt = S.msub[nxp * 8 + 0 + 2 * (u >> 3) + 4 * (v >> 3)];
       if (pt >= 0) wxv = S.offx[(size_t)pt * SHKZ_TC + 8 * (u & 7) + 64 * (v & 7)];
@@ -1005,38 +1030,72 @@ __global__ void __launch_bounds__(256) k_mic_backward16(PoolSystem S, const floa
       const int pt = S.msub[nzp * 8 + (u >> 3) + 2 * (v >> 3)];
       if (pt >= 0) wzv = S.offz[(size_t)pt * SHKZ_TC + (u & 7) + 8 * (v & 7)];
     }
-    ux[tid] = wxv;
-    uy[tid] = wyv;
-    uz[tid] = wzv;
+  }
+  __syncthreads();
+  {
+    // upper weights in place: W?[c] <- the lower weight of the +x/+y/+z
+    // neighbour cell (the macro neighbour's, across the face), so the sweep
+    // reads them at the cell's own index. Thread (jj, kk) owns its x-row; the
+    // y/z shifts read other threads' rows, so all reads precede all writes.
+    const int r0 = MT * jj + MT * MT * kk;
+    float ux[MT], uy[MT], uz[MT];
+    #pragma unroll
+    for (int i = 0; i < MT; ++i) {
+      ux[i] = i < MT - 1 ? WX[r0 + i + 1] : 0.f;
+      uy[i] = jj < MT - 1 ? WY[r0 + i + MT] : 0.f;
+      uz[i] = kk < MT - 1 ? WZ[r0 + i + MT * MT] : 0.f;
+    }
+    __syncthreads();
+    // the +x face weight of row (jj, kk) is entry jj + 16 kk of the +x
+    // neighbour's column, held by thread jj + 16 kk (this thread); the +y
+    // face weight of cell (i, 15, kk) and the +z weight of cell (i, jj, 15)
+    // are entries i + 16 kk and i + 16 jj, gathered through shared memory
+    #pragma unroll
+    for (int i = 0; i < MT; ++i) {
+      WX[r0 + i] = ux[i];
+      WY[r0 + i] = uy[i];
+      WZ[r0 + i] = uz[i];
+    }
+    WX[r0 + MT - 1] = wxv;
+    __syncthreads();
+    {
+      // tid = u + 16 v holds the +y weight of cell (u, 15, v) and the +z
+      // weight of cell (u, v, 15)
+      const int u = tid & 15, v = tid >> 4;
+      WY[u + MT * (MT - 1) + MT * MT * v] = wyv;
+      WZ[u + MT * v + MT * MT * (MT - 1)] = wzv;
+    }
+  }
+  {
+    // downstream faces into the ghost layer (x = 16, y = 16, z = 16); the
+    // weight shifts above overlap the wait for them
+    const int u = tid & 15, v = tid >> 4;
     bool ok = true;
-    hx[tid] = nxp >= 0 ? face_get(faces + ((size_t)nxp * 3 + 0) * 256 + tid, epoch, ok) : 0.0f;
-    hy[tid] = nyp >= 0 ? face_get(faces + ((size_t)nyp * 3 + 1) * 256 + tid, epoch, ok) : 0.0f;
-    hz[tid] = nzp >= 0 ? face_get(faces + ((size_t)nzp * 3 + 2) * 256 + tid, epoch, ok) : 0.0f;
+    Zg[mghost(MT, u, v)] = nxp >= 0 ? face_get(faces + ((size_t)nxp * 3 + 0) * 256 + tid, epoch, ok) : 0.0f;
+    Zg[mghost(u, MT, v)] = nyp >= 0 ? face_get(faces + ((size_t)nyp * 3 + 1) * 256 + tid, epoch, ok) : 0.0f;
+    Zg[mghost(u, v, MT)] = nzp >= 0 ? face_get(faces + ((size_t)nzp * 3 + 2) * 256 + tid, epoch, ok) : 0.0f;
     if (!ok) atomicCAS(&ws->error, 0, slot + 1);
   }
   __syncthreads();
-  for (int s = 3 * MT - 3; s >= 0; --s) {
-    const int ii = s - jj - kk;
-    if (ii >= 0 && ii < MT) {
-      const int c = ii + MT * jj + MT * MT * kk;
-      const float zx = ii < MT - 1 ? Z[c + 1] : hx[jj + MT * kk];
-      const float wx = ii < MT - 1 ? WX[c + 1] : ux[jj + MT * kk];
-      const float zy = jj < MT - 1 ? Z[c + MT] : hy[ii + MT * kk];
-      const float wy = jj < MT - 1 ? WY[c + MT] : uy[ii + MT * kk];
-      const float zz = kk < MT - 1 ? Z[c + MT * MT] : hz[ii + MT * jj];
-      const float wz = kk < MT - 1 ? WZ[c + MT * MT] : uz[ii + MT * jj];
-      Z[c] = Tt[c] + Dd[c] * (wx * zx + wy * zy + wz * zz);
+  {
+    const int cb = 15 * jj + 255 * kk, gb = mghost(0, jj, kk) - jj - kk;
+    for (int s = 3 * MT - 3; s >= 0; --s) {
+      if ((unsigned)(s - jj - kk) < (unsigned)MT) {
+        const int c = s + cb, g = s + gb;
+        const float zx = Zg[g + 1], zy = Zg[g + MGY], zz = Zg[g + MGZ];
+        Zg[g] = Tt[c] + Dd[c] * (WX[c] * zx + WY[c] * zy + WZ[c] * zz);
+      }
+      __syncthreads();
     }
-    __syncthreads();
   }
   {
     unsigned long long *f = faces + (size_t)mt * 3 * 256;
     const int u = tid & 15, v = tid >> 4;
-    face_put(f + 0 * 256 + tid, epoch, Z[MT * u + MT * MT * v]);
-    face_put(f + 1 * 256 + tid, epoch, Z[u + MT * MT * v]);
-    face_put(f + 2 * 256 + tid, epoch, Z[u + MT * v]);
+    face_put(f + 0 * 256 + tid, epoch, Zg[mghost(0, u, v)]);
+    face_put(f + 1 * 256 + tid, epoch, Zg[mghost(u, 0, v)]);
+    face_put(f + 2 * 256 + tid, epoch, Zg[mghost(u, v, 0)]);
   }
-  macro_store(sub, Z, z);
+  macro_store_ghosted(sub, Zg, z);
   // fused z.r over the macro tile's cells (absent sub-tiles contribute zero)
   double dot = 0.0;
   for (int e = tid; e < 8 * 128; e += 256) {
@@ -1045,17 +1104,17 @@ __global__ void __launch_bounds__(256) k_mic_backward16(PoolSystem S, const floa
     if (pt < 0) continue;
     const int c = v * 4;
     const int x = (c & 7) + (stt & 1) * 8, y = ((c >> 3) & 7) + ((stt >> 1) & 1) * 8, zc = (c >> 6) + (stt >> 2) * 8;
-    const float4 zv = *reinterpret_cast<const float4 *>(Z + x + 16 * y + 256 * zc);
+    const int o = mghost(x, y, zc);
     const float4 rv = reinterpret_cast<const float4 *>(r + (size_t)pt * SHKZ_TC)[v];
-    dot += (double)zv.x * rv.x + (double)zv.y * rv.y + (double)zv.z * rv.z + (double)zv.w * rv.w;
+    dot += (double)Zg[o] * rv.x + (double)Zg[o + 1] * rv.y + (double)Zg[o + 2] * rv.z + (double)Zg[o + 3] * rv.w;
   }
   const double tot = block_sum<256>(dot, red);
   if (tid == 0 && partials) partials[mt] = tot;
   sweep_end(ws, epoch);
 }
 
-size_t mic16_smem_forward() { return sizeof(float) * (6 * MTC + 3 * 256); }
-size_t mic16_smem_backward() { return sizeof(float) * (6 * MTC + 6 * 256); }
+size_t mic16_smem_forward() { return sizeof(float) * (MGC + 5 * MTC); }
+size_t mic16_smem_backward() { return sizeof(float) * (MGC + 5 * MTC); }
 
 // ---------------------------------------------------------------------------
 // FP64 residual r64 = b64 - A64 x64 (x64 in FP64), its norms, and the FP32
