@@ -54,6 +54,7 @@ struct shkz_b200_ctx {
          *colsum = nullptr, *dmic64 = nullptr, *x64 = nullptr, *r64 = nullptr, *xref64 = nullptr,
          *p64 = nullptr, *q64 = nullptr, *z64 = nullptr;
   float *x = nullptr, *r = nullptr, *p = nullptr, *q = nullptr, *z = nullptr, *t = nullptr, *p32 = nullptr;
+  float *pb = nullptr;  // second direction buffer: the fused stencil writes the new p beside the old one
   // reductions and wavefront sync
   double *partials = nullptr, *out4 = nullptr;
   unsigned *counter = nullptr;
@@ -225,7 +226,7 @@ static int ensure_pool(shkz_b200_ctx *ctx, int K) {
   GROW(diag64, n); GROW(offx64, n); GROW(offy64, n); GROW(offz64, n); GROW(rhs64, n);
   GROW(colsum, n); GROW(dmic64, n); GROW(x64, n); GROW(r64, n); GROW(xref64, n);
   GROW(p64, n); GROW(q64, n); GROW(z64, n);
-  GROW(x, n); GROW(r, n); GROW(p, n); GROW(q, n); GROW(z, n); GROW(t, n); GROW(p32, n);
+  GROW(x, n); GROW(r, n); GROW(p, n); GROW(q, n); GROW(z, n); GROW(t, n); GROW(p32, n); GROW(pb, n);
   GROW(partials, (size_t)2 * cap + 4 * 8192);
   GROW(wflags, (size_t)cap);
   GROW(faces_f, (size_t)cap * 3 * 64);
@@ -347,7 +348,7 @@ extern "C" void shkz_b200_destroy(shkz_b200_ctx *ctx) {
                   ctx->wflags, ctx->faces_f, ctx->faces_b, ctx->ws, ctx->st_scratch, ctx->mcount, ctx->mstate,
                   ctx->mtile, ctx->mnbr, ctx->msched, ctx->msub, ctx->mfaces_f, ctx->mfaces_b, ctx->curv,
                   ctx->prev, ctx->rank_pool, ctx->rank_cnt, ctx->rank_total, ctx->xw, ctx->h_dens[0],
-                  ctx->h_dens[1], ctx->h_dens[2], ctx->flush};
+                  ctx->h_dens[1], ctx->h_dens[2], ctx->flush, ctx->pb};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (ctx->model) learned_free(ctx->model);
@@ -471,17 +472,24 @@ static int solve_system(shkz_b200_ctx *ctx, double tol, int precond, shkz_b200_r
   SolverState hst;
   int rc = 0, updates = 0;
   bool true_checked = false;
+  // MIC(0) on macro tiles: the direction update p = z + beta p rides in the
+  // next iteration's stencil (ping-pong between two p buffers) and the x/r
+  // update in the forward sweep's staging, so an iteration is three passes
+  // (stencil, forward sweep, backward sweep) plus the rho scalar
+  // (the current direction is in ctx->p after an even number of completed
+  // iterations and in ctx->pb after an odd one; the kernels pick it on the
+  // device, where retired launches leave the count alone)
+  const bool fused = precond == SHKZ_B200_PRECOND_MIC0 && S.KM > 0;
   for (;;) {
     for (int b = 0; b < batch; ++b) {
-      launch_spmv(S, ctx->p, ctx->q, ctx->partials, ctx->counter, ctx->st, 0, s);
-      // MIC(0) on macro tiles: the x/r update rides in the forward sweep's staging
-      if (precond == SHKZ_B200_PRECOND_MIC0 &&
-          launch_mic_apply_update(S, ctx->d32, ctx->r, ctx->t, ctx->z, ctx->partials, ctx->p, ctx->q, ctx->x,
-                                  ctx->counter + 1, ctx->st, max_it, wsync(ctx, 1), wsync(ctx, 2), s)) {
+      if (fused) {
+        launch_spmv_update(S, ctx->p, ctx->pb, ctx->z, ctx->q, ctx->partials, ctx->counter, ctx->st, s);
+        launch_mic_apply_update(S, ctx->d32, ctx->r, ctx->t, ctx->z, ctx->partials, ctx->p, ctx->pb, ctx->q, ctx->x,
+                                ctx->counter + 1, ctx->st, max_it, wsync(ctx, 1), wsync(ctx, 2), s);
         launch_finish_rho(ctx->partials, mic_partial_count(S), ctx->st, 0, s);
-        launch_update_p(n, ctx->z, ctx->p, ctx->st, s);
         continue;
       }
+      launch_spmv(S, ctx->p, ctx->q, ctx->partials, ctx->counter, ctx->st, 0, s);
       launch_update_xr(n, ctx->p, ctx->q, ctx->x, ctx->r, ctx->partials, ctx->counter + 1, ctx->st, max_it, s);
       launch_iteration_tail(ctx, S, n, precond, s);
     }
@@ -505,8 +513,15 @@ static int solve_system(shkz_b200_ctx *ctx, double tol, int precond, shkz_b200_r
     launch_inner_init(n, ctx->r64, 1.0 / scale, ctx->r, ctx->x, s);
     launch_state_resume(ctx->st, kReliableDrop * rmax / scale, s);
     true_checked = false;
-    // complete the interrupted iteration with the replaced residual
-    launch_iteration_tail(ctx, S, n, precond, s);
+    // complete the interrupted iteration with the replaced residual (the
+    // fused loop leaves the direction update to its next stencil)
+    if (fused) {
+      launch_mic_apply(S, ctx->d32, ctx->r, ctx->t, ctx->z, ctx->partials, ctx->faces_f, ctx->faces_b, wsync(ctx, 1),
+                       wsync(ctx, 2), ctx->st, s);
+      launch_finish_rho(ctx->partials, mic_partial_count(S), ctx->st, 0, s);
+    } else {
+      launch_iteration_tail(ctx, S, n, precond, s);
+    }
   }
   if (!true_checked) {
     // plain FP32 finish (refine off) or max iterations: report the true residual

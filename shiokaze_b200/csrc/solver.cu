@@ -182,12 +182,22 @@ struct SpmvSmem {
   float xs[10][10][16];  // (kk+1, jj+1, ii+4); halos at kk/jj 0,9 and ii 3,12
 };
 
+// zu != null: the pending direction update p <- z + beta p is applied on the
+// fly (k_update_p's arithmetic) to the tile and its halo, and the tile's new
+// p is written to pout (a different buffer: other CTAs still read the old p
+// for their halos).
 __device__ __forceinline__ void stage_tile(const PoolSystem &S, const float *__restrict__ p, int pt, SpmvSmem &sm,
-                                           float4 &xv) {
+                                           float4 &xv, const float *__restrict__ zu = nullptr,
+                                           float *__restrict__ pout = nullptr, float beta = 0.0f) {
   const int tid = threadIdx.x;
   const int q4 = tid & 1, jj = (tid >> 1) & 7, kk = tid >> 4;
   const size_t base = (size_t)pt * SHKZ_TC + kk * 64 + jj * 8 + q4 * 4;
   xv = ld4(p + base);
+  if (zu) {
+    const float4 zv = ld4(zu + base);
+    xv.x = zv.x + beta * xv.x; xv.y = zv.y + beta * xv.y; xv.z = zv.z + beta * xv.z; xv.w = zv.w + beta * xv.w;
+    st4(pout + base, xv);
+  }
   st4(&sm.xs[kk + 1][jj + 1][4 + 4 * q4], xv);
   for (int h = tid; h < 384; h += 128) {
     const int face = h >> 6, a = h & 63, u = a & 7, v = a >> 3;
@@ -201,7 +211,12 @@ __device__ __forceinline__ void stage_tile(const PoolSystem &S, const float *__r
       case NB_ZM: cell = u + 8 * v + 64 * 7; break;
       default:    cell = u + 8 * v; break;
     }
-    const float val = nb >= 0 ? p[(size_t)nb * SHKZ_TC + cell] : 0.0f;
+    float val = 0.0f;
+    if (nb >= 0) {
+      const size_t o = (size_t)nb * SHKZ_TC + cell;
+      val = p[o];
+      if (zu) val = zu[o] + beta * val;
+    }
     switch (face) {
       case NB_XM: sm.xs[v + 1][u + 1][3] = val; break;
       case NB_XP: sm.xs[v + 1][u + 1][12] = val; break;
@@ -297,19 +312,30 @@ __device__ __forceinline__ float4 stencil4(const PoolSystem &S, int pt, const Sp
 // mode 0: q = A p and pq = p.q -> st->pq, st->alpha = rho/pq
 // mode 1: q = A p only
 #define SPMV_CTAS_PER_SM 8
-__global__ void __launch_bounds__(128, SPMV_CTAS_PER_SM) k_spmv(PoolSystem S, const float *__restrict__ p, float *__restrict__ q,
-                                              double *partials, unsigned *counter, SolverState *st, int mode) {
+// With zu != null, p and pout are the two direction buffers and the one
+// holding the current direction is chosen by the parity of the completed
+// iteration count on the device, so launches that the loop control retires
+// (done != 0) do not flip it.
+__global__ void __launch_bounds__(128, SPMV_CTAS_PER_SM) k_spmv(PoolSystem S, const float *p, float *__restrict__ q,
+                                              double *partials, unsigned *counter, SolverState *st, int mode,
+                                              const float *__restrict__ zu, float *pout) {
   __shared__ SpmvSmem sm;
   __shared__ double red[4];
   if (st && st->done) return;
   double acc = 0.0;
   const int tid = threadIdx.x;
   const int q4 = tid & 1, jj = (tid >> 1) & 7, kk = tid >> 4;
+  const float beta = zu ? (float)st->beta : 0.0f;
+  if (zu && (st->iter & 1)) {
+    float *t = const_cast<float *>(p);
+    p = pout;
+    pout = t;
+  }
   for (int pt = blockIdx.x; pt < S.K; pt += gridDim.x) {
     float4 xv;
     const Coef4 cf = load_coef4(S, pt);
     __syncthreads();
-    stage_tile(S, p, pt, sm, xv);
+    stage_tile(S, p, pt, sm, xv, zu, pout, beta);
     __syncthreads();
     const float4 y = stencil4(S, pt, sm, xv, cf);
     st4(q + (size_t)pt * SHKZ_TC + kk * 64 + jj * 8 + q4 * 4, y);
@@ -902,6 +928,8 @@ __device__ __forceinline__ void macro_store(const int *sub, const float *srcs, f
 // phase, which overlaps the wait for the upstream faces.
 struct SweepUpdate {
   const float *p, *q;
+  const float *p_alt;  // non-null: p / p_alt are the two direction buffers, the current one
+                       // chosen by the parity of st->iter + 1 (the stencil of this iteration wrote it)
   float *x, *r;
   SolverState *st;
   unsigned *counter;
@@ -926,7 +954,8 @@ __global__ void __launch_bounds__(256) k_mic_forward16(PoolSystem S, const float
   if (fu.st) {
     __shared__ double red[8];
     double m = 0.0, s2 = 0.0;
-    macro_load_update(sub, fu.r, fu.q, fu.p, fu.x, (float)fu.st->alpha, d32, S.offx, S.offy, S.offz, R, Dd, WX, WY,
+    const float *pcur = (fu.p_alt && ((fu.st->iter + 1) & 1)) ? fu.p_alt : fu.p;
+    macro_load_update(sub, fu.r, fu.q, pcur, fu.x, (float)fu.st->alpha, d32, S.offx, S.offy, S.offz, R, Dd, WX, WY,
                       WZ, m, s2);
     m = block_max<256>(m, red);
     s2 = block_sum<256>(s2, red);
@@ -1469,7 +1498,14 @@ void launch_spmv(const PoolSystem &S, const float *p, float *q, double *partials
                  int mode, cudaStream_t s) {
   if (S.K <= 0) return;
   count_launches(1);
-  k_spmv<<<spmv_grid(S.K), 128, 0, s>>>(S, p, q, partials, counter, st, mode);
+  k_spmv<<<spmv_grid(S.K), 128, 0, s>>>(S, p, q, partials, counter, st, mode, nullptr, nullptr);
+}
+
+void launch_spmv_update(const PoolSystem &S, float *p0, float *p1, const float *z, float *q, double *partials,
+                        unsigned *counter, SolverState *st, cudaStream_t s) {
+  if (S.K <= 0) return;
+  count_launches(1);
+  k_spmv<<<spmv_grid(S.K), 128, 0, s>>>(S, p0, q, partials, counter, st, 0, z, p1);
 }
 
 // one wave of resident CTAs looping over the tiles
@@ -1534,8 +1570,8 @@ void launch_mic_apply(const PoolSystem &S, const float *d32, const float *r, flo
 }
 
 bool launch_mic_apply_update(const PoolSystem &S, const float *d32, float *r, float *t, float *z, double *partials,
-                             const float *p, const float *q, float *x, unsigned *counter, SolverState *st,
-                             int max_iterations, void *ws_f, void *ws_b, cudaStream_t s) {
+                             const float *p, const float *p_alt, const float *q, float *x, unsigned *counter,
+                             SolverState *st, int max_iterations, void *ws_f, void *ws_b, cudaStream_t s) {
   if (S.K <= 0 || S.KM <= 0) return false;
   static bool attr[64] = {};
   int dev = 0;
@@ -1547,6 +1583,7 @@ bool launch_mic_apply_update(const PoolSystem &S, const float *d32, float *r, fl
   }
   SweepUpdate fu;
   fu.p = p;
+  fu.p_alt = p_alt;
   fu.q = q;
   fu.x = x;
   fu.r = r;

@@ -11,6 +11,12 @@ void pool_assign(const Geometry &G, const int *tile_count, int K, const int *scr
                  int *pool_tile, int *nbr, int *level_count, int *sched, cudaStream_t s);
 size_t wave_sync_bytes();
 int spmv_grid(int K);
+// q = A p with p = z + beta p_old formed on the fly (beta from st, the pending
+// update of the previous iteration): p_old is p0 after an even number of
+// completed iterations (st->iter) and p1 after an odd one, the new p goes to
+// the other buffer; fused p.q -> alpha as launch_spmv mode 0.
+void launch_spmv_update(const PoolSystem &S, float *p0, float *p1, const float *z, float *q, double *partials,
+                        unsigned *counter, SolverState *st, cudaStream_t s);
 void launch_spmv(const PoolSystem &S, const float *p, float *q, double *partials, unsigned *counter, SolverState *st,
                  int mode, cudaStream_t s);
 void launch_update_xr(int n, const float *p, const float *q, float *x, float *r, double *partials, unsigned *counter,
@@ -28,8 +34,8 @@ void launch_mic_apply(const PoolSystem &S, const float *d32, const float *r, flo
 // launch_update_xr, then z = M^-1 r with the z.r partials). False (nothing
 // launched) when the macro-tile sweeps are not in use.
 bool launch_mic_apply_update(const PoolSystem &S, const float *d32, float *r, float *t, float *z, double *partials,
-                             const float *p, const float *q, float *x, unsigned *counter, SolverState *st,
-                             int max_iterations, void *ws_f, void *ws_b, cudaStream_t s);
+                             const float *p, const float *p_alt, const float *q, float *x, unsigned *counter,
+                             SolverState *st, int max_iterations, void *ws_f, void *ws_b, cudaStream_t s);
 void launch_residual64(const PoolSystem &S, const double *b, const double *x, double *r, double *partials,
                        unsigned *counter, double *out4, cudaStream_t s);
 void launch_inner_init(int n, const double *r64, double inv_scale, float *r32, float *x32, cudaStream_t s);
