@@ -40,17 +40,23 @@ UNIT = "ms/projection"
 
 # Algorithmic bytes per pool cell (cells of 8^3 tiles holding >= 1 unknown)
 # for each kernel, FP32 data: reads + writes of the arrays it must touch once.
+# The MIC(0)-PCG iteration on 16^3 macro tiles runs as two passes:
 ALGO_BYTES = {
-    "spmv": 24,        # x 4 + diag 4 + 3 lower weights 12 + y 4
-    "mic_sweeps": 52,  # forward: r, d, 3 w, write t (24); backward: t, d, 3 w, r, write z (28)
-    "update_xr": 24,   # read p, q, x, r; write x, r
-    "update_p": 12,    # read z, p; write p
+    # stencil with the direction update: read p_old, z, diag, 3 lower
+    # weights; write p_new, q
+    "spmv": 32,
+    # forward sweep with the x/r update: read r q p x d + 3 w, write r x t
+    # (44); backward sweep: read t d 3 w r, write z (28)
+    "mic_sweeps": 72,
+    # the unfused kernels (8^3-tile sweeps, learned preconditioner path)
+    "spmv_plain": 24,        # x, diag, 3 lower weights, y
+    "mic_sweeps_plain": 52,  # forward 24, backward 28
+    "update_xr": 24,         # read p, q, x, r; write x, r
+    "update_p": 12,          # read z, p; write p
 }
 
-# One MIC(0)-PCG iteration as run: stencil 24, forward sweep with the fused
-# x/r update (reads r q p x d + 3 w, writes r x t: 44), backward sweep 28,
-# p update 12.
-ITER_BYTES = 108
+# One fused MIC(0)-PCG iteration: stencil pass 32 + sweep pair 72.
+ITER_BYTES = 104
 
 
 def job_ms_per_projection(elapsed_ms: float, steps: int, world: int, device=None) -> float:
@@ -338,8 +344,9 @@ def main():
     kern = {}
     ms = ctypes.c_double()
     cells = ctypes.c_longlong()
-    for name, which in (("spmv", 0), ("mic_sweeps", 1), ("update_xr", 3), ("update_p", 4),
-                        ("label", 5), ("coeff", 6), ("mic_factor", 7)):
+    fused_kernels = (("spmv", 9), ("mic_sweeps", 10))
+    plain_kernels = (("spmv_plain", 0), ("mic_sweeps_plain", 1), ("update_xr", 3), ("update_p", 4))
+    for name, which in fused_kernels + (("label", 5), ("coeff", 6), ("mic_factor", 7)):
         rc = L.shkz_b200_time_kernel(ctx.handle, which, 30 if which != 7 else 5, ctypes.byref(ms), ctypes.byref(cells))
         if rc != 0:
             kern[name] = {"error": rc}
@@ -350,10 +357,19 @@ def main():
             entry["algo_bytes_per_cell"] = ALGO_BYTES[name]
             entry["achieved_gbs"] = gbs
         kern[name] = entry
+    if any("error" in kern.get(k, {"error": 1}) for k, _ in fused_kernels):
+        # no macro tiles (8^3 sweeps): the iteration runs the unfused kernels
+        for name, which in plain_kernels:
+            if L.shkz_b200_time_kernel(ctx.handle, which, 30, ctypes.byref(ms), ctypes.byref(cells)) == 0:
+                kern[name] = {"ms": ms.value, "cells": cells.value, "algo_bytes_per_cell": ALGO_BYTES[name],
+                              "achieved_gbs": ALGO_BYTES[name] * cells.value / (ms.value * 1e-3) / 1e9}
     peak, peak_kind = measured_peaks()
     traffic = ncu_traffic() or {}
-    names = {"spmv": "k_spmv (7-point stencil q = A p with fused p.q)",
-             "mic_sweeps": "k_mic_forward16 + k_mic_backward16 (MIC(0) wavefront sweeps, fused z.r)",
+    names = {"spmv": "k_spmv (stencil q = A p, p = z + beta p formed on the fly, fused p.q)",
+             "mic_sweeps": "k_mic_forward16 + k_mic_backward16 (MIC(0) wavefront sweeps; x/r update and norms "
+                           "in the forward staging, fused z.r)",
+             "spmv_plain": "k_spmv (stencil q = A p with fused p.q)",
+             "mic_sweeps_plain": "k_mic_forward16 + k_mic_backward16 (plain MIC(0) apply)",
              "update_xr": "k_update_xr (x, r update with inf/2-norms)", "update_p": "k_update_p"}
     rooflines = {}
     for kname, entry in kern.items():
@@ -372,15 +388,20 @@ def main():
     if rooflines:
         dom = max(rooflines, key=lambda k: rooflines[k]["ms"])
         roofline = dict(rooflines[dom])
-        if dom == "mic_sweeps":
-            roofline["note"] = ("wavefront-latency bound: 48 dependent macro-tile levels per sweep at 256^3; "
-                                "the HBM fraction shows how far the dependency chain keeps it from streaming")
+        if dom.startswith("mic_sweeps"):
+            roofline["note"] = ("wavefront-latency bound: each sweep is a chain of dependent macro-tile levels "
+                                "(38 in the 256^3 tank) of 46 diagonal steps each; the HBM fraction shows how far "
+                                "the dependency chain keeps it from streaming")
     ms_it = last["ms_solve"] / max(1, last["iterations"])
-    it_bytes = ITER_BYTES * kern.get("spmv", {}).get("cells", 0)
+    fused = "spmv" in rooflines and "mic_sweeps" in rooflines
+    it_cells = kern.get("spmv" if fused else "spmv_plain", {}).get("cells", 0)
+    it_per_cell = ITER_BYTES if fused else (ALGO_BYTES["spmv_plain"] + ALGO_BYTES["mic_sweeps_plain"] +
+                                            ALGO_BYTES["update_xr"] + ALGO_BYTES["update_p"])
+    it_bytes = it_per_cell * it_cells
     iteration_roofline = {"bytes_per_iteration": it_bytes, "ms_per_iteration": ms_it,
                           "achieved": it_bytes / (ms_it * 1e-3) / 1e9 if ms_it else None, "peak": peak,
                           "unit": "GB/s", "frac": (it_bytes / (ms_it * 1e-3) / 1e9) / peak if ms_it else None,
-                          "algo_bytes_per_cell": ITER_BYTES}
+                          "algo_bytes_per_cell": it_per_cell}
 
     # end to end through the host-buffer C-ABI call with pinned host memory
     e2e = None

@@ -197,11 +197,16 @@ int shkz_b200_apply_matrix(shkz_b200_ctx *ctx, const float *x_cells, float *y_ce
 
 /* Device timing of one kernel on the last projection's system: launches it
  * `reps` times on the context stream, each launch between CUDA events after a
- * 256 MB write that evicts the L2, and stores the mean milliseconds per launch. which: 0 = stencil q = A p with fused p.q,
- * 1 = MIC(0) forward sweep, 2 = MIC(0) backward sweep with fused z.r,
- * 3 = fused x/r update with norms, 4 = p update, 5 = unknown labelling,
- * 6 = weights/rhs assembly, 7 = MIC(0) factor, 8 = one application of the
- * learned preconditioner's network (needs a loaded or initialised network). *cells_out (may be NULL)
+ * 256 MB write that evicts the L2, and stores the mean milliseconds per
+ * launch. which: 0 = stencil q = A p with fused p.q, 1 (or 2) = the MIC(0)
+ * forward and backward sweep pair with fused z.r, 3 = fused x/r update with
+ * norms, 4 = p update, 5 = unknown labelling, 6 = weights/rhs assembly,
+ * 7 = MIC(0) factor, 8 = one application of the learned preconditioner's
+ * network (needs a loaded or initialised network), and the two passes of
+ * the fused MIC(0)-PCG iteration on 16^3 macro tiles: 9 = stencil with the
+ * direction update p = z + beta p, 10 = sweep pair with the x/r update in
+ * the forward sweep (9 and 10 need a MIC(0) projection on macro tiles
+ * first, else SHKZ_B200_ERR_STATE). *cells_out (may be NULL)
  * receives the cells the kernel sweeps per launch (pool cells, or grid cells
  * for 5). No reference counterpart: it is the measurement hook for the
  * roofline figures. */

@@ -1147,10 +1147,18 @@ extern "C" int shkz_b200_time_kernel(shkz_b200_ctx *ctx, int which, int reps, do
       case 7: launch_mic_factor(S, ctx->colsum, ctx->cfg.mic_omega, ctx->cfg.mic_min_diag_ratio, ctx->dmic64,
                                 ctx->d32, ctx->wflags, wsync(ctx, 0), s); break;
       case 8: learned_apply(ctx->model, learned_system(ctx), ctx->r, 1.0, ctx->t, s); break;
+      case 9:
+        launch_spmv_update(S, ctx->p, ctx->pb, ctx->z, ctx->q, ctx->partials, ctx->counter, ctx->st_scratch, s);
+        break;
+      case 10:
+        launch_mic_apply_update(S, ctx->d32, ctx->r, ctx->t, ctx->z, ctx->partials, ctx->p, ctx->pb, ctx->q, ctx->x,
+                                ctx->counter + 1, ctx->st_scratch, 1 << 30, wsync(ctx, 1), wsync(ctx, 2), s);
+        break;
       default: break;
     }
   };
-  if (which < 0 || which > 8) return SHKZ_B200_ERR_ARG;
+  if (which < 0 || which > 10) return SHKZ_B200_ERR_ARG;
+  if (which >= 9 && (!ctx->pb || S.KM <= 0)) return SHKZ_B200_ERR_STATE;
   if (which == 8) {
     const int rc = learned_ready(ctx);
     if (rc) return rc;
