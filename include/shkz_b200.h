@@ -166,6 +166,37 @@ int shkz_b200_project_host(shkz_b200_ctx *ctx, const shkz_b200_project_args *arg
 /* Same, with every array already resident on the context's device. */
 int shkz_b200_project_device(shkz_b200_ctx *ctx, const shkz_b200_project_args *args, shkz_b200_result *out);
 
+/* Velocity extension after a projection: what the liquid solver does right
+ * after project() (macliquid3::extend_both, src/liquid/macliquid3.cpp:330-340)
+ * -- `width` passes of macarray_extrapolator3::extrapolate
+ * (include/shiokaze/array/macarray_extrapolator3.h: each inactive face next
+ * to an active one takes the mean of its active neighbours and becomes
+ * active), then, when constrain != 0, macutility3::constrain_velocity
+ * (src/utility/macutility3.cpp:61-92: no flow into the solid at faces inside
+ * it, none out through the domain's floor and ceiling). Same grid layouts as
+ * shkz_b200_project_args; solid / solid_active (nodes) may be NULL for no
+ * solid. Results are bit-identical to the reference's. nx, ny, nz >= 2,
+ * 0 <= width <= 4096. */
+typedef struct shkz_b200_extend_args {
+  int nx, ny, nz;
+  double dx;
+  int width;                      /* extrapolation passes */
+  int constrain;                  /* 1: constrain_velocity after the passes */
+  const float *solid;             /* nodes, may be NULL */
+  const uint8_t *solid_active;    /* nodes, may be NULL */
+  float *velocity[3];             /* faces, in/out */
+  uint8_t *velocity_active[3];    /* faces, in/out */
+} shkz_b200_extend_args;
+
+/* Host buffers (copied to the device and back). */
+int shkz_b200_extend_velocity_host(shkz_b200_ctx *ctx, const shkz_b200_extend_args *args);
+
+/* Device pointers on the context's device, e.g. the arrays just passed to
+ * shkz_b200_project_device: the velocity stays on the GPU between the
+ * projection and its extension. The masks and the solid arrays must start on
+ * 16-byte boundaries (cudaMalloc's are), else SHKZ_B200_ERR_ARG. */
+int shkz_b200_extend_velocity_device(shkz_b200_ctx *ctx, const shkz_b200_extend_args *args);
+
 /* The CUDA stream the context launches on (as an opaque pointer), so callers
  * can order their own work against it. */
 void *shkz_b200_stream(shkz_b200_ctx *ctx);

@@ -17,6 +17,12 @@
 //   HarnessDensity=<file>      set_solid_density() with face densities read
 //                              from <file> (double, x-fastest, dim 0..2)
 //   HarnessVolume=<cur>:<tgt>  set_target_volume(cur, tgt) before each call
+//   HarnessExtend=w            after the last projection, extend the velocity
+//                              w layers with macarray_extrapolator3::extrapolate
+//                              (include/shiokaze/array/macarray_extrapolator3.h)
+//   HarnessConstrain=1         then macutility3::constrain_velocity(solid, velocity)
+//                              (src/utility/macutility3.cpp:61-92), as
+//                              macliquid3::extend_both does (src/liquid/macliquid3.cpp:330-340)
 //
 // Input file (little endian):
 //   char[8] "SHKZIN01"; int32 nx,ny,nz, has_solid, has_solid_velocity;
@@ -32,6 +38,8 @@
 #include <shiokaze/array/array3.h>
 #include <shiokaze/array/macarray3.h>
 #include <shiokaze/projection/macproject3_interface.h>
+#include <shiokaze/utility/macutility3_interface.h>
+#include <shiokaze/array/macarray_extrapolator3.h>
 #include <shiokaze/core/configuration.h>
 #include <shiokaze/core/credit.h>
 #include <cstdio>
@@ -53,6 +61,8 @@ public:
 	harness_root() {
 		m_macproject.set_environment("shape",&m_shape);
 		m_macproject.set_environment("dx",&m_dx);
+		m_macutility.set_environment("shape",&m_shape);
+		m_macutility.set_environment("dx",&m_dx);
 	}
 	shape3 m_shape;
 	double m_dx {1.0};
@@ -62,6 +72,7 @@ public:
 	macarray3<Real> m_solid_velocity{this};
 	macarray3<Real> m_density{this};
 	macproject3_driver m_macproject{this,"macpressuresolver3"};
+	macutility3_driver m_macutility{this,"macutility3"};
 };
 }
 //
@@ -217,6 +228,14 @@ int main( int argc, const char *argv[] ) {
 		root.m_macproject->project(dt,velocity,solid,solid_velocity,fluid,kappa);
 		auto t1 = std::chrono::steady_clock::now();
 		best_ms = std::min(best_ms,std::chrono::duration<double,std::milli>(t1-t0).count());
+	}
+	//
+	if( dict.count("HarnessExtend") ) {
+		const int width = std::atoi(dict["HarnessExtend"].c_str());
+		if( width > 0 ) macarray_extrapolator3::extrapolate<Real>(velocity,width);
+		if( dict.count("HarnessConstrain") && std::atoi(dict["HarnessConstrain"].c_str()) ) {
+			root.m_macutility->constrain_velocity(solid,velocity);
+		}
 	}
 	//
 	const array3<Real> &pressure = *root.m_macproject->get_pressure();

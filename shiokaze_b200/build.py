@@ -30,6 +30,7 @@ UNITS = {
     "api.cu": [],
     "noalloc.cu": [],
     "warmstart.cu": [],
+    "extend.cu": ["-fmad=false"],
 }
 HEADERS = ["common.cuh", "kernels.h", "solver.h", "learned.h", "tc_conv.cuh"]
 

@@ -88,6 +88,10 @@ struct shkz_b200_ctx {
   int cap_warm_pool = 0;
   size_t cap_rank_cnt = 0;
   float *h_dens[3] = {};           // staging of the solid density faces (host path)
+  float *ext_v[3] = {};            // velocity extension: side buffer of new values per component
+  uint8_t *ext_a[3] = {};          // and its flags
+  size_t cap_ext[3] = {0, 0, 0};
+  int *ext_flag = nullptr;         // levelset_exist(solid) of the extension's constraint
   void *flush = nullptr;           // 256 MB written between timed kernel launches (> L2)
   size_t cap_h_dens[3] = {0, 0, 0};
 };
@@ -348,7 +352,8 @@ extern "C" void shkz_b200_destroy(shkz_b200_ctx *ctx) {
                   ctx->wflags, ctx->faces_f, ctx->faces_b, ctx->ws, ctx->st_scratch, ctx->mcount, ctx->mstate,
                   ctx->mtile, ctx->mnbr, ctx->msched, ctx->msub, ctx->mfaces_f, ctx->mfaces_b, ctx->curv,
                   ctx->prev, ctx->rank_pool, ctx->rank_cnt, ctx->rank_total, ctx->xw, ctx->h_dens[0],
-                  ctx->h_dens[1], ctx->h_dens[2], ctx->flush, ctx->pb};
+                  ctx->h_dens[1], ctx->h_dens[2], ctx->flush, ctx->pb, ctx->ext_v[0], ctx->ext_v[1], ctx->ext_v[2],
+                  ctx->ext_a[0], ctx->ext_a[1], ctx->ext_a[2], ctx->ext_flag};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (ctx->model) learned_free(ctx->model);
@@ -895,6 +900,121 @@ extern "C" int shkz_b200_project_host(shkz_b200_ctx *ctx, const shkz_b200_projec
   res->ms_total = ms_between(e0, e3);
   res->status = rc;
   return rc;
+}
+
+// --------------------------------------------------------------------------
+// Velocity extension after a projection (macliquid3::extend_both,
+// src/liquid/macliquid3.cpp:330-340): kernels in extend.cu.
+
+static int validate_extend(const shkz_b200_extend_args *a) {
+  if (!a || a->nx < 2 || a->ny < 2 || a->nz < 2) return SHKZ_B200_ERR_ARG;
+  if (a->nx > 65536 || a->ny > 65536 || a->nz > 65536) return SHKZ_B200_ERR_LIMIT;
+  if ((size_t)a->nx * a->ny * a->nz > ((size_t)1 << 31)) return SHKZ_B200_ERR_LIMIT;
+  if (a->width < 0 || a->width > 4096) return SHKZ_B200_ERR_ARG;
+  if (a->constrain && !(a->dx > 0.0)) return SHKZ_B200_ERR_ARG;
+  if ((a->solid == nullptr) != (a->solid_active == nullptr)) return SHKZ_B200_ERR_ARG;
+  for (int d = 0; d < 3; ++d)
+    if (!a->velocity[d] || !a->velocity_active[d]) return SHKZ_B200_ERR_ARG;
+  // the kernels read masks 16 bytes and the solid 4 values at a time
+  auto aligned16 = [](const void *p) { return ((uintptr_t)p & 15u) == 0; };
+  for (int d = 0; d < 3; ++d)
+    if (!aligned16(a->velocity_active[d])) return SHKZ_B200_ERR_ARG;
+  if (a->solid && !(aligned16(a->solid) && aligned16(a->solid_active))) return SHKZ_B200_ERR_ARG;
+  return 0;
+}
+
+static int extend_device(shkz_b200_ctx *ctx, const shkz_b200_extend_args *a) {
+  cudaStream_t s = ctx->stream;
+  size_t nf[3];
+  for (int d = 0; d < 3; ++d) {
+    nf[d] = (size_t)(a->nx + (d == 0)) * (a->ny + (d == 1)) * (a->nz + (d == 2));
+    if (nf[d] > ctx->cap_ext[d]) {
+      GROW(ext_v[d], nf[d]);
+      GROW(ext_a[d], nf[d]);
+      ctx->cap_ext[d] = nf[d];
+    }
+  }
+  if (!ctx->ext_flag) GROW(ext_flag, 1);
+  // ext_v / ext_a are a side buffer and its flags; the flags start (and end) zero
+  for (int d = 0; d < 3; ++d) SHKZ_CUDA_TRY(cudaMemsetAsync(ctx->ext_a[d], 0, nf[d], s));
+  for (int d = 0; d < 3; ++d) {
+    const int W = a->nx + (d == 0), H = a->ny + (d == 1), D = a->nz + (d == 2);
+    for (int w = 0; w < a->width; ++w)
+      launch_extrapolate(W, H, D, a->velocity[d], a->velocity_active[d], ctx->ext_v[d], ctx->ext_a[d], s);
+  }
+  if (a->constrain) {
+    ConstrainFields f;
+    for (int d = 0; d < 3; ++d) {
+      f.save[d] = a->velocity[d];
+      f.act[d] = a->velocity_active[d];
+    }
+    SHKZ_CUDA_TRY(cudaMemsetAsync(ctx->ext_flag, 0, sizeof(int), s));
+    if (a->solid) {
+      const size_t nodes = (size_t)(a->nx + 1) * (a->ny + 1) * (a->nz + 1);
+      launch_solid_exists(a->solid, a->solid_active, nodes, ctx->ext_flag, s);
+    }
+    // all three components are found on the unchanged field, then committed
+    for (int d = 0; d < 3; ++d)
+      launch_constrain_find(d, a->nx, a->ny, a->nz, a->dx, a->solid, ctx->ext_flag, f, ctx->ext_v[d], ctx->ext_a[d], s);
+    for (int d = 0; d < 3; ++d) launch_apply_side(nf[d], a->velocity[d], ctx->ext_v[d], ctx->ext_a[d], s);
+  }
+  SHKZ_CUDA_TRY(cudaGetLastError());
+  SHKZ_CUDA_TRY(cudaStreamSynchronize(s));
+  return 0;
+}
+
+extern "C" int shkz_b200_extend_velocity_device(shkz_b200_ctx *ctx, const shkz_b200_extend_args *a) {
+  if (!ctx) return SHKZ_B200_ERR_ARG;
+  int rc = validate_extend(a);
+  if (rc) return rc;
+  cudaSetDevice(ctx->device);
+  return extend_device(ctx, a);
+}
+
+extern "C" int shkz_b200_extend_velocity_host(shkz_b200_ctx *ctx, const shkz_b200_extend_args *a) {
+  if (!ctx || !a) return SHKZ_B200_ERR_ARG;
+  // host arrays may have any alignment: they are staged into the context's buffers
+  shkz_b200_extend_args chk = *a;
+  static const float f16[4] __attribute__((aligned(16))) = {0.f, 0.f, 0.f, 0.f};
+  static const uint8_t b16[16] __attribute__((aligned(16))) = {};
+  for (int d = 0; d < 3; ++d)
+    if (chk.velocity_active[d]) chk.velocity_active[d] = const_cast<uint8_t *>(b16);
+  if (chk.solid) {
+    chk.solid = f16;
+    chk.solid_active = chk.solid_active ? b16 : nullptr;
+  }
+  int rc = validate_extend(&chk);
+  if (rc) return rc;
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  const Geometry G = make_geometry(a->nx, a->ny, a->nz);
+  const bool svel[3] = {false, false, false};
+  rc = ensure_host_staging(ctx, G, a->solid != nullptr, svel);
+  if (rc) return rc;
+  const size_t nodes = (size_t)(a->nx + 1) * (a->ny + 1) * (a->nz + 1);
+  shkz_b200_extend_args da = *a;
+  if (a->solid) {
+    SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->h_solid, a->solid, nodes * 4, cudaMemcpyHostToDevice, s));
+    SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->h_solid_active, a->solid_active, nodes, cudaMemcpyHostToDevice, s));
+    da.solid = ctx->h_solid;
+    da.solid_active = ctx->h_solid_active;
+  }
+  size_t nf[3];
+  for (int d = 0; d < 3; ++d) {
+    nf[d] = (size_t)(a->nx + (d == 0)) * (a->ny + (d == 1)) * (a->nz + (d == 2));
+    SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->h_vel[d], a->velocity[d], nf[d] * 4, cudaMemcpyHostToDevice, s));
+    SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->h_vact[d], a->velocity_active[d], nf[d], cudaMemcpyHostToDevice, s));
+    da.velocity[d] = ctx->h_vel[d];
+    da.velocity_active[d] = ctx->h_vact[d];
+  }
+  rc = extend_device(ctx, &da);
+  if (rc) return rc;
+  for (int d = 0; d < 3; ++d) {
+    SHKZ_CUDA_TRY(cudaMemcpyAsync(a->velocity[d], ctx->h_vel[d], nf[d] * 4, cudaMemcpyDeviceToHost, s));
+    SHKZ_CUDA_TRY(cudaMemcpyAsync(a->velocity_active[d], ctx->h_vact[d], nf[d], cudaMemcpyDeviceToHost, s));
+  }
+  SHKZ_CUDA_TRY(cudaStreamSynchronize(s));
+  return 0;
 }
 
 // --------------------------------------------------------------------------

@@ -46,6 +46,19 @@ void launch_coeff(const AssemblyInputs &in, const int *flags, const int *pool_ti
                   const CoeffOutputs &out, cudaStream_t s);
 void launch_velocity_update(const AssemblyInputs &in, const int *flags, const int *tile_state,
                             const float *pressure_pool, float *const vel[3], uint8_t *const vact[3], cudaStream_t s);
+// velocity extension after a projection (extend.cu)
+struct ConstrainFields {
+  const float *save[3];    // the velocity components (read-only while the constraint is found)
+  const uint8_t *act[3];   // their active masks
+};
+// one extrapolation pass in place: frontier values into side/flag, then committed
+// (flag must be all zero on entry and is all zero again on return)
+void launch_extrapolate(int W, int H, int D, float *v, uint8_t *a, float *side, uint8_t *flag, cudaStream_t s);
+void launch_solid_exists(const float *solid, const uint8_t *act, size_t n, int *flag, cudaStream_t s);
+// constrained values of component d that differ from the field, into side/flag
+void launch_constrain_find(int d, int nx, int ny, int nz, double dx, const float *solid, const int *solid_flag,
+                           const ConstrainFields &f, float *side, uint8_t *flag, cudaStream_t s);
+void launch_apply_side(size_t n, float *v, const float *side, uint8_t *flag, cudaStream_t s);
 void launch_surface_tension(const AssemblyInputs &in, const int *flags, float *curv, double kappa, float *const vel[3],
                             const uint8_t *const vact[3], cudaStream_t s);
 void launch_scatter_pressure(const Geometry &G, const int *tile_state, const float *pressure_pool, const uint8_t *unk,

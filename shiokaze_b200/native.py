@@ -62,6 +62,15 @@ class ProjectArgs(ctypes.Structure):
     ]
 
 
+class ExtendArgs(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("dx", ctypes.c_double),
+        ("width", ctypes.c_int), ("constrain", ctypes.c_int),
+        ("solid", ctypes.c_void_p), ("solid_active", ctypes.c_void_p),
+        ("velocity", ctypes.c_void_p * 3), ("velocity_active", ctypes.c_void_p * 3),
+    ]
+
+
 class Result(ctypes.Structure):
     _fields_ = [
         ("status", ctypes.c_int), ("iterations", ctypes.c_int), ("outer_steps", ctypes.c_int),
@@ -88,7 +97,7 @@ EXPORTS = [
     "shkz_b200_learned_save", "shkz_b200_learned_load", "shkz_b200_conv3d", "shkz_b200_conv3d_noalloc",
     "shkz_b200_set_target_volume", "shkz_b200_get_volume_state", "shkz_b200_set_volume_state",
     "shkz_b200_warm_start_size", "shkz_b200_get_warm_start", "shkz_b200_set_warm_start",
-    "shkz_b200_learned_flops",
+    "shkz_b200_learned_flops", "shkz_b200_extend_velocity_host", "shkz_b200_extend_velocity_device",
 ]
 
 _lib = None
@@ -114,6 +123,8 @@ def load(path: str = LIB_PATH):
     L.shkz_b200_last_error.restype = ctypes.c_char_p
     L.shkz_b200_project_host.argtypes = [P, ctypes.POINTER(ProjectArgs), ctypes.POINTER(Result)]
     L.shkz_b200_project_device.argtypes = [P, ctypes.POINTER(ProjectArgs), ctypes.POINTER(Result)]
+    L.shkz_b200_extend_velocity_host.argtypes = [P, ctypes.POINTER(ExtendArgs)]
+    L.shkz_b200_extend_velocity_device.argtypes = [P, ctypes.POINTER(ExtendArgs)]
     L.shkz_b200_stream.argtypes = [P]
     L.shkz_b200_stream.restype = P
     L.shkz_b200_solve_csr.argtypes = [P, ctypes.c_longlong, P, P, P, P, P, ctypes.POINTER(Result)]
@@ -200,3 +211,30 @@ class Context:
     @property
     def stream(self) -> int:
         return load().shkz_b200_stream(self.handle)
+
+
+def extend_velocity(ctx: Context, velocity, velocity_active, solid, solid_active, dx: float, width: int,
+                    constrain: bool = True):
+    """The velocity extension the liquid solver runs right after a projection
+    (macliquid3::extend_both, src/liquid/macliquid3.cpp:330-340), on host
+    numpy grids through ``shkz_b200_extend_velocity_host``: ``width``
+    extrapolation passes, then (``constrain``) constrain_velocity. Face grids
+    are [k, j, i] float32 with uint8 masks; solid is the nodal level set (or
+    None). Returns new (velocity, velocity_active) lists."""
+    import numpy as np
+    vel = [np.ascontiguousarray(v, np.float32).copy() for v in velocity]
+    act = [np.ascontiguousarray(m, np.uint8).copy() for m in velocity_active]
+    nz, ny, nx = vel[0].shape[0], vel[0].shape[1], vel[0].shape[2] - 1
+    a = ExtendArgs()
+    a.nx, a.ny, a.nz, a.dx, a.width, a.constrain = nx, ny, nz, float(dx), int(width), int(bool(constrain))
+    keep = []
+    if solid is not None:
+        s = np.ascontiguousarray(solid, np.float32)
+        sa = np.ascontiguousarray(solid_active, np.uint8)
+        keep += [s, sa]
+        a.solid, a.solid_active = s.ctypes.data, sa.ctypes.data
+    for d in range(3):
+        a.velocity[d] = vel[d].ctypes.data
+        a.velocity_active[d] = act[d].ctypes.data
+    ctx.check(load().shkz_b200_extend_velocity_host(ctx.handle, ctypes.byref(a)), "shkz_b200_extend_velocity_host")
+    return vel, act

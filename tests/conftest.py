@@ -18,11 +18,12 @@ def pytest_configure(config):
 
 def golden_names(prefix: str = ""):
     """Fixtures of plain projections, or (prefix "term_") of projections with
-    one optional term on."""
+    one optional term on, or (prefix "ext_") of the velocity extension after a
+    projection."""
     names = sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz"))
     if prefix:
         return [n for n in names if n.startswith(prefix)]
-    return [n for n in names if not n.startswith("term_")]
+    return [n for n in names if not n.startswith(("term_", "ext_"))]
 
 
 def load_golden(name):
@@ -64,6 +65,11 @@ def golden(request):
 
 @pytest.fixture(params=golden_names("term_") if os.path.isdir(GOLDEN) else [])
 def golden_term(request):
+    return request.param, load_golden(request.param)
+
+
+@pytest.fixture(params=golden_names("ext_") if os.path.isdir(GOLDEN) else [])
+def golden_ext(request):
     return request.param, load_golden(request.param)
 
 

@@ -124,6 +124,37 @@ def make_term(name: str, build) -> str:
     return path
 
 
+# Velocity extension after the projection (macliquid3::extend_both,
+# src/liquid/macliquid3.cpp:330-340): the reference's projected velocity, and
+# the same after macarray_extrapolator3::extrapolate(width) and (when on)
+# macutility3::constrain_velocity.
+EXTEND_CASES = {
+    "ext_sloshing_tank_24": lambda: (scenes.sloshing_tank(n=24, seed=1, tol=1e-6), 3, 1),
+    "ext_dambreak_sphere_24": lambda: (scenes.dambreak_sphere(n=24, seed=7), 4, 1),
+    "ext_splash_24": lambda: (scenes.splash(n=24, seed=4, spheres=12), 2, 0),
+}
+
+
+def make_extend(name: str, build) -> str:
+    sc, width, constrain = build()
+    r0 = ref_runner.run_reference(sc, mode="mic0", dump_system=False)
+    r1 = ref_runner.run_reference(sc, mode="mic0", dump_system=False,
+                                  extra={"HarnessExtend": width, "HarnessConstrain": constrain})
+    payload = dict(
+        shape=np.array([sc.nx, sc.ny, sc.nz], np.int32), dx=np.float64(sc.dx),
+        width=np.int32(width), constrain=np.int32(constrain), has_solid=np.int32(sc.solid_phi is not None),
+        solid=r0.solid.astype(np.float32), solid_active=r0.solid_active,
+        u0=r0.velocity[0].astype(np.float32), v0=r0.velocity[1].astype(np.float32),
+        w0=r0.velocity[2].astype(np.float32),
+        u0_active=r0.velocity_active[0], v0_active=r0.velocity_active[1], w0_active=r0.velocity_active[2],
+        u=r1.velocity[0].astype(np.float32), v=r1.velocity[1].astype(np.float32), w=r1.velocity[2].astype(np.float32),
+        u_active=r1.velocity_active[0], v_active=r1.velocity_active[1], w_active=r1.velocity_active[2],
+    )
+    path = os.path.join(OUT, f"{name}.npz")
+    np.savez_compressed(path, **payload)
+    return path
+
+
 def main():
     if not ref_runner.ref_available("float"):
         raise SystemExit("compiled reference not found: run `make -C oracle/ref` first")
@@ -137,6 +168,11 @@ def main():
         if only and name not in only:
             continue
         p = make_term(name, build)
+        print(p, os.path.getsize(p))
+    for name, build in EXTEND_CASES.items():
+        if only and name not in only:
+            continue
+        p = make_extend(name, build)
         print(p, os.path.getsize(p))
 
 
