@@ -21,6 +21,9 @@
 //                              w layers with macarray_extrapolator3::extrapolate
 //                              (include/shiokaze/array/macarray_extrapolator3.h)
 //   HarnessConstrain=1         then macutility3::constrain_velocity(solid, velocity)
+//   Projection=<module>        any projection module (default macpressuresolver3;
+//                              macstreamfuncsolver3 has no pressure grid, which is
+//                              then written as empty)
 //                              (src/utility/macutility3.cpp:61-92), as
 //                              macliquid3::extend_both does (src/liquid/macliquid3.cpp:330-340)
 //
@@ -71,6 +74,7 @@ public:
 	macarray3<Real> m_velocity{this};
 	macarray3<Real> m_solid_velocity{this};
 	macarray3<Real> m_density{this};
+	array3<Real> m_no_pressure{this};
 	macproject3_driver m_macproject{this,"macpressuresolver3"};
 	macutility3_driver m_macutility{this,"macutility3"};
 };
@@ -238,8 +242,14 @@ int main( int argc, const char *argv[] ) {
 		}
 	}
 	//
-	const array3<Real> &pressure = *root.m_macproject->get_pressure();
-	dump_cells(pressure,shape);
+	// a projection without a pressure grid (macstreamfuncsolver3::get_pressure
+	// returns nullptr) is written as an empty, inactive grid
+	const array3<Real> *pressure_ptr = root.m_macproject->get_pressure();
+	if( ! pressure_ptr ) {
+		root.m_no_pressure.initialize(shape);
+		pressure_ptr = &root.m_no_pressure;
+	}
+	dump_cells(*pressure_ptr,shape);
 	for( int dim=0; dim<3; ++dim ) dump_cells(velocity[dim],shape.face(dim));
 	wr(out,&best_ms,1);
 	std::fclose(out);

@@ -89,3 +89,26 @@ def test_pcg_b200_matches_reference_pcg(n, seed, tol):
     for d in range(3):
         np.testing.assert_array_equal(got.velocity_active[d], ref.velocity_active[d])
         assert rel_inf(got.velocity[d], ref.velocity[d]) <= tol_p
+
+
+@pytest.mark.skipif(not (ref_runner.ref_available("float") and os.path.exists(PCG_PLUGIN)),
+                    reason="needs the compiled reference harness and the pcg_b200 module")
+@pytest.mark.parametrize("n,seed,tol", [(24, 7, 1e-4), (32, 2, 1e-6)])
+def test_streamfunc_projection_runs_on_pcg_b200(n, seed, tol):
+    """The reference's other projection, macstreamfuncsolver3 (a vector-potential
+    solve, src/projection/macstreamfuncsolver3.cpp), takes its linear solver
+    from the same LinSolver plugin: with LinSolver=pcg_b200 its solves run on
+    the GPU, and its projected velocity matches the one it gets from the
+    reference's pcg."""
+    sc = scenes.dambreak_sphere(n=n, seed=seed, tol=tol)
+    extra = {"Projection": "macstreamfuncsolver3"}
+    ref = ref_runner.run_reference(sc, linsolver="pcg", dump_system=False, extra=extra)
+    got = ref_runner.run_reference(sc, linsolver="pcg_b200", dump_system=False, extra=extra, extra_libpath=[PKG])
+    vin = sc.velocity_effective()
+    tol_v = max(1e-5, 10 * tol)
+    for d in range(3):
+        np.testing.assert_array_equal(got.velocity_active[d], ref.velocity_active[d])
+        # the projection did change the field, and both solvers agree on it
+        m = ref.velocity_active[d] != 0
+        assert np.abs(ref.velocity[d][m] - vin[d][m]).max() > 1e-2
+        assert rel_inf(got.velocity[d], ref.velocity[d]) <= tol_v, (d, rel_inf(got.velocity[d], ref.velocity[d]))
