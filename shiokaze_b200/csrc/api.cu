@@ -480,7 +480,8 @@ static int solve_system(shkz_b200_ctx *ctx, double tol, int precond, shkz_b200_r
   // MIC(0) on macro tiles: the direction update p = z + beta p rides in the
   // next iteration's stencil (ping-pong between two p buffers) and the x/r
   // update in the forward sweep's staging, so an iteration is three passes
-  // (stencil, forward sweep, backward sweep) plus the rho scalar
+  // (stencil, forward sweep, backward sweep; the backward sweep's last CTA
+  // also finishes rho and beta)
   // (the current direction is in ctx->p after an even number of completed
   // iterations and in ctx->pb after an odd one; the kernels pick it on the
   // device, where retired launches leave the count alone)
@@ -490,8 +491,7 @@ static int solve_system(shkz_b200_ctx *ctx, double tol, int precond, shkz_b200_r
       if (fused) {
         launch_spmv_update(S, ctx->p, ctx->pb, ctx->z, ctx->q, ctx->partials, ctx->counter, ctx->st, s);
         launch_mic_apply_update(S, ctx->d32, ctx->r, ctx->t, ctx->z, ctx->partials, ctx->p, ctx->pb, ctx->q, ctx->x,
-                                ctx->counter + 1, ctx->st, max_it, wsync(ctx, 1), wsync(ctx, 2), s);
-        launch_finish_rho(ctx->partials, mic_partial_count(S), ctx->st, 0, s);
+                                ctx->counter + 1, ctx->st, max_it, wsync(ctx, 1), wsync(ctx, 2), ctx->counter + 5, s);
         continue;
       }
       launch_spmv(S, ctx->p, ctx->q, ctx->partials, ctx->counter, ctx->st, 0, s);
@@ -1272,7 +1272,8 @@ extern "C" int shkz_b200_time_kernel(shkz_b200_ctx *ctx, int which, int reps, do
         break;
       case 10:
         launch_mic_apply_update(S, ctx->d32, ctx->r, ctx->t, ctx->z, ctx->partials, ctx->p, ctx->pb, ctx->q, ctx->x,
-                                ctx->counter + 1, ctx->st_scratch, 1 << 30, wsync(ctx, 1), wsync(ctx, 2), s);
+                                ctx->counter + 1, ctx->st_scratch, 1 << 30, wsync(ctx, 1), wsync(ctx, 2),
+                                ctx->counter + 5, s);
         break;
       default: break;
     }

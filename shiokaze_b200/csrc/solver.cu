@@ -1028,7 +1028,7 @@ __global__ void __launch_bounds__(256) k_mic_backward16(PoolSystem S, const floa
                                                         const float *__restrict__ t, const float *__restrict__ r,
                                                         float *__restrict__ z, double *partials,
                                                         unsigned long long *faces, WaveSync *ws,
-                                                        const SolverState *st) {
+                                                        SolverState *st, unsigned *finish) {
   extern __shared__ __align__(16) float smb[];
   float *Zg = smb, *Tt = Zg + MGC, *Dd = Tt + MTC, *WX = Dd + MTC, *WY = WX + MTC, *WZ = WY + MTC;
   __shared__ int sub[8];
@@ -1139,6 +1139,16 @@ __global__ void __launch_bounds__(256) k_mic_backward16(PoolSystem S, const floa
   }
   const double tot = block_sum<256>(dot, red);
   if (tid == 0 && partials) partials[mt] = tot;
+  if (finish && last_block(finish)) {
+    // k_finish_rho of the PCG iteration: rho_new = z.r from the macro-tile
+    // partials in tile order, beta = rho_new / rho
+    const double rho_new = sum_partials<256>(partials, S.KM, red);
+    if (tid == 0) {
+      st->beta = rho_new / st->rho;
+      st->rho = rho_new;
+      *finish = 0;
+    }
+  }
   sweep_end(ws, epoch);
 }
 
@@ -1560,7 +1570,8 @@ void launch_mic_apply(const PoolSystem &S, const float *d32, const float *r, flo
     k_mic_forward16<<<S.KM, 256, mic16_smem_forward(), s>>>(S, d32, r, t, S.mfaces_f, (WaveSync *)ws_f, st,
                                                              SweepUpdate{});
     k_mic_backward16<<<S.KM, 256, mic16_smem_backward(), s>>>(S, d32, t, r, z, partials, S.mfaces_b,
-                                                               (WaveSync *)ws_b, st);
+                                                               (WaveSync *)ws_b, const_cast<SolverState *>(st),
+                                                               nullptr);
     return;
   }
   count_launches(1);
@@ -1571,7 +1582,8 @@ void launch_mic_apply(const PoolSystem &S, const float *d32, const float *r, flo
 
 bool launch_mic_apply_update(const PoolSystem &S, const float *d32, float *r, float *t, float *z, double *partials,
                              const float *p, const float *p_alt, const float *q, float *x, unsigned *counter,
-                             SolverState *st, int max_iterations, void *ws_f, void *ws_b, cudaStream_t s) {
+                             SolverState *st, int max_iterations, void *ws_f, void *ws_b, unsigned *finish,
+                             cudaStream_t s) {
   if (S.K <= 0 || S.KM <= 0) return false;
   static bool attr[64] = {};
   int dev = 0;
@@ -1594,7 +1606,7 @@ bool launch_mic_apply_update(const PoolSystem &S, const float *d32, float *r, fl
   count_launches(2);
   k_mic_forward16<<<S.KM, 256, mic16_smem_forward(), s>>>(S, d32, r, t, S.mfaces_f, (WaveSync *)ws_f, st, fu);
   k_mic_backward16<<<S.KM, 256, mic16_smem_backward(), s>>>(S, d32, t, r, z, partials, S.mfaces_b, (WaveSync *)ws_b,
-                                                             st);
+                                                             st, finish);
   return true;
 }
 

@@ -32,10 +32,13 @@ void launch_mic_apply(const PoolSystem &S, const float *d32, const float *r, flo
 // One PCG iteration's x/r update fused into the MIC(0) application on 16^3
 // macro tiles (r -= alpha q, x += alpha p, norms and stopping bookkeeping as
 // launch_update_xr, then z = M^-1 r with the z.r partials). False (nothing
-// launched) when the macro-tile sweeps are not in use.
+// launched) when the macro-tile sweeps are not in use. finish (may be null): a
+// zeroed counter; the backward sweep's last CTA then also computes
+// rho_new = z.r, beta = rho_new / rho, rho = rho_new (k_finish_rho's update).
 bool launch_mic_apply_update(const PoolSystem &S, const float *d32, float *r, float *t, float *z, double *partials,
                              const float *p, const float *p_alt, const float *q, float *x, unsigned *counter,
-                             SolverState *st, int max_iterations, void *ws_f, void *ws_b, cudaStream_t s);
+                             SolverState *st, int max_iterations, void *ws_f, void *ws_b, unsigned *finish,
+                             cudaStream_t s);
 void launch_residual64(const PoolSystem &S, const double *b, const double *x, double *r, double *partials,
                        unsigned *counter, double *out4, cudaStream_t s);
 void launch_inner_init(int n, const double *r64, double inv_scale, float *r32, float *x32, cudaStream_t s);
