@@ -347,7 +347,11 @@ def main():
     fused_kernels = (("spmv", 9), ("mic_sweeps", 10))
     plain_kernels = (("spmv_plain", 0), ("mic_sweeps_plain", 1), ("update_xr", 3), ("update_p", 4))
     for name, which in fused_kernels + (("label", 5), ("coeff", 6), ("mic_factor", 7)):
+        # each timing loop in an NVTX range "time_kernel_<name>", so that a
+        # profiler can select its launches (ncu --nvtx --nvtx-include ...)
+        torch.cuda.nvtx.range_push(f"time_kernel_{name}")
         rc = L.shkz_b200_time_kernel(ctx.handle, which, 30 if which != 7 else 5, ctypes.byref(ms), ctypes.byref(cells))
+        torch.cuda.nvtx.range_pop()
         if rc != 0:
             kern[name] = {"error": rc}
             continue
