@@ -270,10 +270,9 @@ __device__ __forceinline__ Coef4 load_coef4(const PoolSystem &S, int pt) {
 }
 
 // Computes the four outputs of this thread for tile pt (after staging and a barrier).
-__device__ __forceinline__ float4 stencil4(const PoolSystem &S, int pt, const SpmvSmem &sm, float4 xv, const Coef4 &cf) {
+__device__ __forceinline__ float4 stencil4(const SpmvSmem &sm, float4 xv, const Coef4 &cf) {
   const int tid = threadIdx.x;
   const int q4 = tid & 1, jj = (tid >> 1) & 7, kk = tid >> 4;
-  const size_t base = (size_t)pt * SHKZ_TC + kk * 64 + jj * 8 + q4 * 4;
   const float4 dg = cf.dg, ox = cf.ox, oy = cf.oy, oz = cf.oz;
   // upper weights: lower weights of the +x/+y/+z neighbour cells
   const float oxn = __shfl_down_sync(0xffffffffu, ox.x, 1);
@@ -337,7 +336,7 @@ __global__ void __launch_bounds__(128, SPMV_CTAS_PER_SM) k_spmv(PoolSystem S, co
     __syncthreads();
     stage_tile(S, p, pt, sm, xv, zu, pout, beta);
     __syncthreads();
-    const float4 y = stencil4(S, pt, sm, xv, cf);
+    const float4 y = stencil4(sm, xv, cf);
     st4(q + (size_t)pt * SHKZ_TC + kk * 64 + jj * 8 + q4 * 4, y);
     acc += (double)xv.x * y.x + (double)xv.y * y.y + (double)xv.z * y.z + (double)xv.w * y.w;
   }
