@@ -624,17 +624,26 @@ __device__ __forceinline__ void face_put(unsigned long long *e, int epoch, float
   const unsigned long long w = ((unsigned long long)(unsigned)epoch << 32) | (unsigned long long)__float_as_uint(v);
   asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(e), "l"(w) : "memory");
 }
-// Bounded wait for the entry of the current epoch; returns its value (0 and
-// *ok = false when the limit was hit).
-__device__ __forceinline__ float face_get(const unsigned long long *e, int epoch, bool &ok) {
-  for (int it = 0; it < SPIN_LIMIT; ++it) {
-    unsigned long long w;
-    asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(w) : "l"(e) : "memory");
-    if ((int)(w >> 32) == epoch) return __uint_as_float((unsigned)(w & 0xffffffffu));
+// The three upstream (downstream) face entries of one thread, polled
+// together: every round issues the loads of the entries still missing before
+// it checks any of them, so once the last face lands the thread sees it one
+// L2 round trip later, not one per face. e0/e1/e2 null: no neighbour (0).
+__device__ __forceinline__ void face_get3(const unsigned long long *e0, const unsigned long long *e1,
+                                          const unsigned long long *e2, int epoch, float &v0, float &v1, float &v2,
+                                          bool &ok) {
+  bool r0 = !e0, r1 = !e1, r2 = !e2;
+  v0 = v1 = v2 = 0.0f;
+  for (int it = 0; it < SPIN_LIMIT && !(r0 && r1 && r2); ++it) {
+    unsigned long long w0 = 0ull, w1 = 0ull, w2 = 0ull;
+    if (!r0) asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(w0) : "l"(e0) : "memory");
+    if (!r1) asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(w1) : "l"(e1) : "memory");
+    if (!r2) asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(w2) : "l"(e2) : "memory");
+    if (!r0 && (int)(w0 >> 32) == epoch) { v0 = __uint_as_float((unsigned)(w0 & 0xffffffffu)); r0 = true; }
+    if (!r1 && (int)(w1 >> 32) == epoch) { v1 = __uint_as_float((unsigned)(w1 & 0xffffffffu)); r1 = true; }
+    if (!r2 && (int)(w2 >> 32) == epoch) { v2 = __uint_as_float((unsigned)(w2 & 0xffffffffu)); r2 = true; }
     if (it > 32) __nanosleep(32);
   }
-  ok = false;
-  return 0.0f;
+  if (!(r0 && r1 && r2)) ok = false;
 }
 
 __device__ __forceinline__ void sweep_begin(WaveSync *ws, int &slot, int &epoch) {
@@ -681,9 +690,9 @@ __global__ void __launch_bounds__(64) k_mic_forward(PoolSystem S, const int *sch
   {
     const int nxm = S.nbr[pt * 6 + NB_XM], nym = S.nbr[pt * 6 + NB_YM], nzm = S.nbr[pt * 6 + NB_ZM];
     bool ok = true;
-    hx[tid] = nxm >= 0 ? face_get(faces + ((size_t)nxm * 3 + 0) * 64 + tid, epoch, ok) : 0.0f;
-    hy[tid] = nym >= 0 ? face_get(faces + ((size_t)nym * 3 + 1) * 64 + tid, epoch, ok) : 0.0f;
-    hz[tid] = nzm >= 0 ? face_get(faces + ((size_t)nzm * 3 + 2) * 64 + tid, epoch, ok) : 0.0f;
+    face_get3(nxm >= 0 ? faces + ((size_t)nxm * 3 + 0) * 64 + tid : nullptr,
+              nym >= 0 ? faces + ((size_t)nym * 3 + 1) * 64 + tid : nullptr,
+              nzm >= 0 ? faces + ((size_t)nzm * 3 + 2) * 64 + tid : nullptr, epoch, hx[tid], hy[tid], hz[tid], ok);
     if (!ok) atomicCAS(&ws->error, 0, slot + 1);
   }
   __syncthreads();
@@ -739,9 +748,9 @@ __global__ void __launch_bounds__(64) k_mic_backward(PoolSystem S, const int *sc
     uy[tid] = nyp >= 0 ? S.offy[(size_t)nyp * SHKZ_TC + u + 64 * v] : 0.0f;
     uz[tid] = nzp >= 0 ? S.offz[(size_t)nzp * SHKZ_TC + u + 8 * v] : 0.0f;
     bool ok = true;
-    hx[tid] = nxp >= 0 ? face_get(faces + ((size_t)nxp * 3 + 0) * 64 + tid, epoch, ok) : 0.0f;
-    hy[tid] = nyp >= 0 ? face_get(faces + ((size_t)nyp * 3 + 1) * 64 + tid, epoch, ok) : 0.0f;
-    hz[tid] = nzp >= 0 ? face_get(faces + ((size_t)nzp * 3 + 2) * 64 + tid, epoch, ok) : 0.0f;
+    face_get3(nxp >= 0 ? faces + ((size_t)nxp * 3 + 0) * 64 + tid : nullptr,
+              nyp >= 0 ? faces + ((size_t)nyp * 3 + 1) * 64 + tid : nullptr,
+              nzp >= 0 ? faces + ((size_t)nzp * 3 + 2) * 64 + tid : nullptr, epoch, hx[tid], hy[tid], hz[tid], ok);
     if (!ok) atomicCAS(&ws->error, 0, slot + 1);
   }
   __syncthreads();
@@ -970,9 +979,13 @@ __global__ void __launch_bounds__(256) k_mic_forward16(PoolSystem S, const float
     const int nxm = S.mnbr[mt * 6 + NB_XM], nym = S.mnbr[mt * 6 + NB_YM], nzm = S.mnbr[mt * 6 + NB_ZM];
     const int u = tid & 15, v = tid >> 4;
     bool ok = true;
-    Tg[mghost(-1, u, v)] = nxm >= 0 ? face_get(faces + ((size_t)nxm * 3 + 0) * 256 + tid, epoch, ok) : 0.0f;
-    Tg[mghost(u, -1, v)] = nym >= 0 ? face_get(faces + ((size_t)nym * 3 + 1) * 256 + tid, epoch, ok) : 0.0f;
-    Tg[mghost(u, v, -1)] = nzm >= 0 ? face_get(faces + ((size_t)nzm * 3 + 2) * 256 + tid, epoch, ok) : 0.0f;
+    float gx, gy, gz;
+    face_get3(nxm >= 0 ? faces + ((size_t)nxm * 3 + 0) * 256 + tid : nullptr,
+              nym >= 0 ? faces + ((size_t)nym * 3 + 1) * 256 + tid : nullptr,
+              nzm >= 0 ? faces + ((size_t)nzm * 3 + 2) * 256 + tid : nullptr, epoch, gx, gy, gz, ok);
+    Tg[mghost(-1, u, v)] = gx;
+    Tg[mghost(u, -1, v)] = gy;
+    Tg[mghost(u, v, -1)] = gz;
     if (!ok) atomicCAS(&ws->error, 0, slot + 1);
   }
   __syncthreads();
@@ -1099,9 +1112,13 @@ __global__ void __launch_bounds__(256) k_mic_backward16(PoolSystem S, const floa
     // weight shifts above overlap the wait for them
     const int u = tid & 15, v = tid >> 4;
     bool ok = true;
-    Zg[mghost(MT, u, v)] = nxp >= 0 ? face_get(faces + ((size_t)nxp * 3 + 0) * 256 + tid, epoch, ok) : 0.0f;
-    Zg[mghost(u, MT, v)] = nyp >= 0 ? face_get(faces + ((size_t)nyp * 3 + 1) * 256 + tid, epoch, ok) : 0.0f;
-    Zg[mghost(u, v, MT)] = nzp >= 0 ? face_get(faces + ((size_t)nzp * 3 + 2) * 256 + tid, epoch, ok) : 0.0f;
+    float gx, gy, gz;
+    face_get3(nxp >= 0 ? faces + ((size_t)nxp * 3 + 0) * 256 + tid : nullptr,
+              nyp >= 0 ? faces + ((size_t)nyp * 3 + 1) * 256 + tid : nullptr,
+              nzp >= 0 ? faces + ((size_t)nzp * 3 + 2) * 256 + tid : nullptr, epoch, gx, gy, gz, ok);
+    Zg[mghost(MT, u, v)] = gx;
+    Zg[mghost(u, MT, v)] = gy;
+    Zg[mghost(u, v, MT)] = gz;
     if (!ok) atomicCAS(&ws->error, 0, slot + 1);
   }
   __syncthreads();
