@@ -163,11 +163,13 @@ def cpu_reference_sample(n: int = 128):
     from oracle import ref_runner
     sc = scenes.sloshing_tank(n=n, seed=0, tol=1e-6)
     if ref_runner.ref_available("float"):
-        r = ref_runner.run_reference(sc, mode="mic0", dump_system=True)
+        # no system dump: the reference's solver would write it inside project()
+        r = ref_runner.run_reference(sc, mode="mic0", dump_system=False)
+        its = r.console_solves[-1][0] if r.console_solves else None
         return {"value": r.projection_ms, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
                 "sample": f"sloshing tank {n}^3 (1/{(256 // n) ** 3} of the 256^3 cells), reference "
                           f"macpressuresolver3 + MIC(0)-PCG to 1e-6, Threads={os.cpu_count()} (its PCG is "
-                          f"single-threaded), {r.iterations} iterations, 1 projection"}
+                          f"single-threaded), {its} iterations, 1 projection"}
     from oracle import oracle
     t = time.perf_counter()
     o = oracle.project(sc, mic0=True)
@@ -191,9 +193,10 @@ def run_reference_arm(args):
     t_start = time.perf_counter()
     while len(times) < max(1, args.steps):
         if kind == "reference":
-            r = ref_runner.run_reference(sc, mode="mic0", dump_system=True)
+            # no system dump: the reference's solver would write it inside project()
+            r = ref_runner.run_reference(sc, mode="mic0", dump_system=False)
             times.append(r.projection_ms)
-            iters = r.iterations
+            iters = r.console_solves[-1][0] if r.console_solves else None
         else:
             from oracle import oracle
             t = time.perf_counter()
