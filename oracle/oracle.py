@@ -57,6 +57,9 @@ def lib():
                                 ctypes.c_double, ctypes.c_double, P]
         L.shkzo_update_velocity.argtypes = [ctypes.c_int] * 3 + [ctypes.c_double, ctypes.c_double, P, P, P, P, P, P,
                                                                 P]
+        L.shkzo_splat.restype = ctypes.c_int
+        L.shkzo_splat.argtypes = [ctypes.c_int] * 3 + [ctypes.c_double, ctypes.c_longlong, P] + \
+            [ctypes.c_int] * 7 + [P] * 5
         _lib = L
     return _lib
 
@@ -263,3 +266,25 @@ def project(scene, tol: Optional[float] = None, mic0: bool = True, tile: int = 8
                         pressure_active=mask.astype(np.uint8), velocity=vel, velocity_active=vact,
                         solve_s=t2 - t1, total_s=t3 - t0, volume_rhs_correct=rhs_add, y_prev=y_prev,
                         warm_prev=x.copy() if x0 is not None else None)
+
+
+def splat(nx: int, ny: int, nz: int, dx: float, particles: np.ndarray, velocity: list, velocity_active: list,
+          apic: bool = True, splat_bullet: bool = False):
+    """FLIP splat and combined grid velocity (``shkzo_splat``) on particle
+    records in the reference's layout (``shiokaze_b200.scenes.PARTICLE_DTYPE``).
+    Returns (velocity, velocity_active, mass, momentum, splat_active), lists of
+    three face grids; the inputs are not modified."""
+    P = np.ascontiguousarray(particles)
+    dt = P.dtype
+    vel = [np.ascontiguousarray(v, np.float32).copy() for v in velocity]
+    act = [np.ascontiguousarray(a, np.uint8).copy() for a in velocity_active]
+    mass = [np.zeros_like(v) for v in vel]
+    mom = [np.zeros_like(v) for v in vel]
+    sact = [np.zeros_like(a) for a in act]
+    off = lambda k: dt.fields[k][1]
+    rc = lib().shkzo_splat(nx, ny, nz, dx, len(P), _p(P), dt.itemsize, off("p"), off("velocity"), off("mass"),
+                           off("c") if apic else -1, off("bullet"), int(splat_bullet),
+                           _ptr3(vel), _ptr3(act), _ptr3(mass), _ptr3(mom), _ptr3(sact))
+    if rc:
+        raise MemoryError("shkzo_splat")
+    return vel, act, mass, mom, sact

@@ -120,3 +120,45 @@ def run_reference(scene, variant: str = "float", mode: str = "mic0", tol: Option
         if dump_system and os.path.exists(dump + ".system.bin"):
             res.system = read_system(dump + ".system.bin")
         return res
+
+
+def run_reference_splat(nx: int, ny: int, nz: int, dx: float, particles: np.ndarray, velocity: list,
+                        velocity_active: list, apic: bool = True, splat_bullet: bool = False,
+                        time: float = 0.0, variant: str = "float") -> dict:
+    """Run the compiled reference FLIP splat (``shkz_ref_splat``: macnbflip3::splat
+    then the combined grid velocity of macflipliquid3) on particle records in
+    the reference's layout. Returns face grids (lists over dim) under
+    ``mass``, ``momentum``, ``splat_active``, ``velocity``, ``velocity_active``."""
+    exe = os.path.join(REF_DIR, variant, "shkz_ref_splat")
+    P = np.ascontiguousarray(particles)
+    n = len(P)
+    with tempfile.TemporaryDirectory() as td:
+        fin, fout = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
+        with open(fin, "wb") as f:
+            f.write(b"SHKZSP01")
+            f.write(struct.pack("<3i2dq", nx, ny, nz, dx, time, n))
+            f.write(np.ascontiguousarray(P["p"], np.float32).tobytes())
+            f.write(np.ascontiguousarray(P["c"], np.float32).tobytes())
+            f.write(np.ascontiguousarray(P["velocity"], np.float32).tobytes())
+            f.write(np.ascontiguousarray(P["mass"], np.float32).tobytes())
+            f.write((np.asarray(P["bullet"]) != 0).astype(np.uint8).tobytes())
+            for v, a in zip(velocity, velocity_active):
+                f.write(np.ascontiguousarray(v, np.float32).tobytes())
+                f.write(np.ascontiguousarray(a, np.uint8).tobytes())
+        env = dict(os.environ)
+        env["LD_LIBRARY_PATH"] = ":".join([os.path.join(REF_DIR, variant), env.get("LD_LIBRARY_PATH", "")])
+        args = [exe, fin, fout, "APIC=" + ("Yes" if apic else "No"),
+                "SplatBulletParticle=" + ("Yes" if splat_bullet else "No")]
+        proc = subprocess.run(args, cwd=td, env=env, capture_output=True, text=True)
+        if proc.returncode != 0:
+            raise RuntimeError(f"reference splat failed ({proc.returncode}):\n{proc.stdout[-2000:]}\n{proc.stderr[-2000:]}")
+        out = {k: [] for k in ("mass", "momentum", "splat_active", "velocity", "velocity_active")}
+        with open(fout, "rb") as f:
+            for d in range(3):
+                shp = (nz + (d == 2), ny + (d == 1), nx + (d == 0))
+                nf = int(np.prod(shp))
+                for k, dt_ in (("mass", np.float32), ("momentum", np.float32), ("splat_active", np.uint8),
+                               ("velocity", np.float32), ("velocity_active", np.uint8)):
+                    w = np.dtype(dt_).itemsize
+                    out[k].append(np.frombuffer(f.read(w * nf), dtype=dt_).reshape(shp).copy())
+    return out

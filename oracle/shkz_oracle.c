@@ -553,3 +553,165 @@ void shkzo_update_velocity(int nx, int ny, int nz, double dx, double dt, const f
                 }
     }
 }
+
+/* ------------------------------------------------------------------------
+ * FLIP splat before the projection.
+ *
+ * Particles are records of `stride` bytes in the reference's layout
+ * (macnbflip3::Particle, src/flip/macnbflip3.h:128-139): float p[3] at
+ * off_p, float velocity[3] at off_v, float mass at off_m, float c[3][3] at
+ * off_c (off_c < 0: APIC off), char bullet at off_bullet (< 0: none).
+ *
+ * Restates, with the reference's operation order and types:
+ *   - the edge hash  pointgridhash3::sort_points, EDGE_MODE
+ *                    (src/pointgridhash/pointgridhash3.cpp:90-100): every
+ *                    particle goes, in index order, into the bucket
+ *                    shape3::find_edge(p/dx, dim) (include/shiokaze/math/
+ *                    shape.h:748-750: (p/dx) rounded to float, + 0.5 off the
+ *                    edge axis rounded to float, truncated, clamped)
+ *   - macnbflip3::splat (src/flip/macnbflip3.cpp:103-148): faces touched by
+ *                    a splatting particle (8 per dim, clamped to the CELL
+ *                    shape) are activated; each then sums over
+ *                    get_face_neighbors(face, dim) (pointgridhash3.cpp:
+ *                    218-231), whose loops run ri, rj, rk over {0,1} for all
+ *                    three axes, so along the face's own axis each bucket is
+ *                    visited twice and every particle is counted twice
+ *   - the combined grid velocity (src/liquid/macflipliquid3.cpp:135-151).
+ * Outputs: mass/momentum/splat_active per face (the splat grid; faces with
+ * zero mass are switched off), velocity/velocity_active updated in place. */
+static inline float rd_f(const unsigned char *rec, int off, int k)
+{
+    float v;
+    memcpy(&v, rec + off + 4 * k, 4);
+    return v;
+}
+
+static inline int edge_axis(float pc, double dx, int half, int extent)
+{
+    const float q = (float)((double)pc / dx);
+    const float t = (float)((double)q + (half ? 0.5 : 0.0));
+    return clampi((int)t, 0, extent - 1);
+}
+
+static inline double tent(double r, double dx)
+{
+    const double x = fabs(r) / dx;
+    const double v = 1.0 - x;
+    return 0.0 < v ? v : 0.0;
+}
+
+int shkzo_splat(int nx, int ny, int nz, double dx, long long count, const void *particles, int stride,
+                int off_p, int off_v, int off_m, int off_c, int off_bullet, int splat_bullet,
+                float *velocity[3], unsigned char *velocity_active[3],
+                float *mass[3], float *momentum[3], unsigned char *splat_active[3])
+{
+    const unsigned char *base = (const unsigned char *)particles;
+    const int n3[3] = {nx, ny, nz};
+    for (int d = 0; d < 3; ++d) {
+        const int fw = face_w(nx, d), fh = face_h(ny, d), fd = face_d(nz, d);
+        const size_t nf = (size_t)fw * fh * fd;
+        int E[3];
+        for (int c = 0; c < 3; ++c) E[c] = n3[c] + (c != d);
+        const size_t ne = (size_t)E[0] * E[1] * E[2];
+        /* edge buckets as a counting sort that keeps index order */
+        long long *start = (long long *)calloc(ne + 1, sizeof(long long));
+        long long *key = (long long *)malloc(sizeof(long long) * (count ? count : 1));
+        long long *list = (long long *)malloc(sizeof(long long) * (count ? count : 1));
+        if (!start || !key || !list) { free(start); free(key); free(list); return -1; }
+        for (long long n = 0; n < count; ++n) {
+            const unsigned char *rec = base + (size_t)n * stride;
+            int e[3];
+            for (int c = 0; c < 3; ++c) e[c] = edge_axis(rd_f(rec, off_p, c), dx, c != d, E[c]);
+            key[n] = (long long)IDX(e[0], e[1], e[2], E[0], E[1]);
+            start[key[n] + 1]++;
+        }
+        for (size_t b = 0; b < ne; ++b) start[b + 1] += start[b];
+        {
+            long long *fill = (long long *)malloc(sizeof(long long) * (ne ? ne : 1));
+            if (!fill) { free(start); free(key); free(list); return -1; }
+            memcpy(fill, start, sizeof(long long) * ne);
+            for (long long n = 0; n < count; ++n) list[fill[key[n]]++] = n;
+            free(fill);
+        }
+        /* activation (macnbflip3.cpp:109-120) */
+        memset(splat_active[d], 0, nf);
+        for (long long n = 0; n < count; ++n) {
+            const unsigned char *rec = base + (size_t)n * stride;
+            if (!splat_bullet && off_bullet >= 0 && rec[off_bullet]) continue;
+            int pi[3];
+            for (int c = 0; c < 3; ++c) pi[c] = (int)((double)rd_f(rec, off_p, c) / dx - 0.5 * (d != c));
+            for (int ii = 0; ii <= 1; ++ii)
+                for (int jj = 0; jj <= 1; ++jj)
+                    for (int kk = 0; kk <= 1; ++kk) {
+                        const int i = clampi(pi[0] + ii, 0, nx - 1);
+                        const int j = clampi(pi[1] + jj, 0, ny - 1);
+                        const int k = clampi(pi[2] + kk, 0, nz - 1);
+                        splat_active[d][IDX(i, j, k, fw, fh)] = 1;
+                    }
+        }
+        /* gather (macnbflip3.cpp:121-143) */
+        for (int k = 0; k < fd; ++k)
+            for (int j = 0; j < fh; ++j)
+                for (int i = 0; i < fw; ++i) {
+                    const size_t f = IDX(i, j, k, fw, fh);
+                    mass[d][f] = 0.0f;
+                    momentum[d][f] = 0.0f;
+                    if (!splat_active[d][f]) continue;
+                    const int fi[3] = {i, j, k};
+                    double pos[3];
+                    for (int c = 0; c < 3; ++c) pos[c] = ((double)fi[c] + 0.5 * (d != c)) * dx;
+                    float mom = 0.0f, m = 0.0f;
+                    for (int dir = -1; dir <= 0; ++dir)
+                        for (int ri = 0; ri <= 1; ++ri)
+                            for (int rj = 0; rj <= 1; ++rj)
+                                for (int rk = 0; rk <= 1; ++rk) {
+                                    const int r3[3] = {ri, rj, rk};
+                                    int q[3];
+                                    int out = 0;
+                                    for (int c = 0; c < 3; ++c) {
+                                        q[c] = fi[c] + (c != d) * r3[c] + (c == d) * dir;
+                                        out |= q[c] < 0 || q[c] >= E[c];
+                                    }
+                                    if (out) continue;
+                                    const size_t b = IDX(q[0], q[1], q[2], E[0], E[1]);
+                                    for (long long s = start[b]; s < start[b + 1]; ++s) {
+                                        const unsigned char *rec = base + (size_t)list[s] * stride;
+                                        if (!splat_bullet && off_bullet >= 0 && rec[off_bullet]) continue;
+                                        float r[3];
+                                        for (int c = 0; c < 3; ++c) r[c] = (float)((double)rd_f(rec, off_p, c) - pos[c]);
+                                        const double w = tent(r[0], dx) * tent(r[1], dx) * tent(r[2], dx);
+                                        if (w != 0.0) {
+                                            const double pm = (double)rd_f(rec, off_m, 0);
+                                            mom = (float)((double)mom + w * pm * (double)rd_f(rec, off_v, d));
+                                            m = (float)((double)m + w * pm);
+                                            if (off_c >= 0) {
+                                                double dot = 0.0;
+                                                for (int c = 0; c < 3; ++c)
+                                                    dot += (double)rd_f(rec, off_c, 3 * d + c) *
+                                                           (pos[c] - (double)rd_f(rec, off_p, c));
+                                                mom = (float)((double)mom + w * pm * dot);
+                                            }
+                                        }
+                                    }
+                                }
+                    if (m != 0.0f) {
+                        mass[d][f] = m;
+                        momentum[d][f] = mom;
+                    } else {
+                        splat_active[d][f] = 0;
+                    }
+                }
+        free(start); free(key); free(list);
+        /* combined grid velocity (macflipliquid3.cpp:141-150) */
+        for (size_t f = 0; f < nf; ++f) {
+            if (!splat_active[d][f]) continue;
+            const double gm64 = 1.0 - (double)mass[d][f];
+            const float gm = velocity_active[d][f] ? (float)(0.0 < gm64 ? gm64 : 0.0) : 0.0f;
+            const float num = gm * velocity[d][f] + momentum[d][f];
+            const float den = gm + mass[d][f];
+            velocity[d][f] = num / den;
+            velocity_active[d][f] = 1;
+        }
+    }
+    return 0;
+}

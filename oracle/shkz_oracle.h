@@ -30,6 +30,10 @@ int shkzo_pcg(long long n, const long long *indptr, const long long *indices, co
 void shkzo_update_velocity(int nx, int ny, int nz, double dx, double dt, const float *pressure,
                            float *const area[3], float *const rho[3], float *const solid_velocity[3],
                            float *velocity[3], unsigned char *velocity_active[3], float *const density[3]);
+int shkzo_splat(int nx, int ny, int nz, double dx, long long count, const void *particles, int stride,
+                int off_p, int off_v, int off_m, int off_c, int off_bullet, int splat_bullet,
+                float *velocity[3], unsigned char *velocity_active[3],
+                float *mass[3], float *momentum[3], unsigned char *splat_active[3]);
 #ifdef __cplusplus
 }
 #endif

@@ -333,6 +333,75 @@ def analytic_sphere(n: int, r: float = 0.4, band_cells: float = 2.0):
     return sc, np.broadcast_to(exact, (n, n, n)).copy()
 
 
+# FLIP particle records in the reference's own layout (macnbflip3::Particle,
+# src/flip/macnbflip3.h:128-139: vec3r p; vec3r c[3]; vec3r velocity; Real
+# mass, r; char bullet; Real bullet_time, sizing_value; unsigned live_count),
+# 84 bytes each; the splat reads p, c, velocity, mass and bullet.
+PARTICLE_DTYPE = np.dtype({
+    "names": ["p", "c", "velocity", "mass", "r", "bullet", "bullet_time", "sizing_value", "live_count"],
+    "formats": [("<f4", (3,)), ("<f4", (3, 3)), ("<f4", (3,)), "<f4", "<f4", "u1", "<f4", "<f4", "<u4"],
+    "offsets": [0, 12, 48, 60, 64, 68, 72, 76, 80],
+    "itemsize": 84,
+})
+
+
+def flip_particles(scene: Scene, per_cell: int = 8, seed: int = 0, bullet_fraction: float = 0.02,
+                   edge_cases: bool = True, band: Optional[float] = None) -> np.ndarray:
+    """Seeded FLIP particles for a scene: ``per_cell`` jittered particles in
+    every liquid cell (effective level set < 0; with ``band``, only cells whose
+    analytic level set is above ``-band * dx``, the narrow band macnbflip3
+    keeps particles in: Narrowband = 3 cells by default, macnbflip3.h:108, at
+    8 to 12 particles per cell, mass 1/8 each), a smooth velocity field plus
+    noise, APIC matrices of a few 1/s, masses around the reference's default
+    1/8 (macnbflip3.cpp:42) and a fraction flagged bullet. With
+    ``edge_cases``, also particles exactly on cell faces and nodes, one float
+    step either side of them, and particles pushed up to 0.45 cells outside
+    the domain on every side (collisions leave such particles in the
+    reference too)."""
+    rng = np.random.default_rng(seed)
+    dx = scene.dx
+    phi = scene.fluid_effective()
+    inside = phi < 0
+    if band is not None:
+        inside &= scene.fluid_phi > -band * dx   # the analytic (unbanded) level set
+    k, j, i = np.nonzero(inside)
+    cells = np.repeat(np.stack([i, j, k], 1), per_cell, axis=0).astype(np.float64)
+    pos = (cells + rng.random(cells.shape)) * dx
+    extra = []
+    if edge_cases and len(cells):
+        n3 = np.array([scene.nx, scene.ny, scene.nz], np.float64)
+        pick = cells[rng.integers(0, len(cells), 96)]
+        on = np.floor(pick) * dx
+        on[:32, 1:] += 0.5 * dx
+        extra.append(on)
+        f = on.astype(np.float32)
+        extra.append(np.nextafter(f, np.float32(np.inf)).astype(np.float64))
+        extra.append(np.nextafter(f, np.float32(-np.inf)).astype(np.float64))
+        for axis in range(3):
+            for side in (0, 1):
+                q = pos[rng.integers(0, len(pos), 16)].copy()
+                off = rng.random(16) * 0.45 * dx
+                q[:, axis] = -off if side == 0 else n3[axis] * dx + off
+                extra.append(q)
+    if extra:
+        pos = np.concatenate([pos] + extra, 0)
+    n = len(pos)
+    P = np.zeros(n, PARTICLE_DTYPE)
+    P["p"] = pos.astype(np.float32)
+    x, y, z = (pos[:, a] for a in range(3))
+    vel = np.stack([0.6 * np.sin(2 * np.pi * y) * np.cos(np.pi * z),
+                    -0.8 * np.sin(np.pi * x) + 0.3 * np.cos(2 * np.pi * z),
+                    0.4 * np.cos(2 * np.pi * x) * np.sin(np.pi * y)], 1)
+    vel += 0.05 * rng.standard_normal(vel.shape)
+    P["velocity"] = vel.astype(np.float32)
+    P["c"] = (2.0 * rng.standard_normal((n, 3, 3))).astype(np.float32)
+    P["mass"] = (0.125 * rng.uniform(0.5, 1.5, n)).astype(np.float32)
+    P["r"] = np.float32(0.25 * dx)
+    P["bullet"] = (rng.random(n) < bullet_fraction).astype(np.uint8)
+    P["live_count"] = rng.integers(0, 8, n).astype(np.uint32)
+    return P
+
+
 SCENES = {
     "dambreak_sphere": dambreak_sphere,
     "sloshing_tank": sloshing_tank,

@@ -19,11 +19,11 @@ def pytest_configure(config):
 def golden_names(prefix: str = ""):
     """Fixtures of plain projections, or (prefix "term_") of projections with
     one optional term on, or (prefix "ext_") of the velocity extension after a
-    projection."""
+    projection, or (prefix "splat_") of the FLIP splat before one."""
     names = sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz"))
     if prefix:
         return [n for n in names if n.startswith(prefix)]
-    return [n for n in names if not n.startswith(("term_", "ext_"))]
+    return [n for n in names if not n.startswith(("term_", "ext_", "splat_"))]
 
 
 def load_golden(name):
@@ -71,6 +71,17 @@ def golden_term(request):
 @pytest.fixture(params=golden_names("ext_") if os.path.isdir(GOLDEN) else [])
 def golden_ext(request):
     return request.param, load_golden(request.param)
+
+
+@pytest.fixture(params=golden_names("splat_") if os.path.isdir(GOLDEN) else [])
+def golden_splat(request):
+    return request.param, load_golden(request.param)
+
+
+def splat_particles(g):
+    """The particle records of a splat_ fixture as a structured array."""
+    from shiokaze_b200.scenes import PARTICLE_DTYPE
+    return np.ascontiguousarray(g["particles"]).view(PARTICLE_DTYPE).reshape(-1)
 
 
 def term_options(g):

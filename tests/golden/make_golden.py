@@ -155,6 +155,36 @@ def make_extend(name: str, build) -> str:
     return path
 
 
+# FLIP splat before the projection (macflipliquid3.cpp:135-151): seeded
+# particles in the reference's record layout over a scene's grid velocity,
+# and what macnbflip3::splat and the combined grid velocity make of them.
+# name: scene, particles per liquid cell, bullet fraction, APIC, SplatBulletParticle
+SPLAT_CASES = {
+    "splat_dambreak_sphere_16": lambda: (scenes.dambreak_sphere(n=16, seed=3), 8, 0.02, True, False),
+    "splat_sloshing_tank_16": lambda: (scenes.sloshing_tank(n=16, seed=2, tol=1e-6), 4, 0.05, False, True),
+    "splat_splash_20": lambda: (scenes.splash(n=20, seed=4, spheres=8), 3, 0.10, True, True),
+}
+
+
+def make_splat(name: str, build) -> str:
+    sc, per_cell, bullets, apic, splat_bullet = build()
+    P = scenes.flip_particles(sc, per_cell=per_cell, seed=11, bullet_fraction=bullets)
+    vel, vact = sc.velocity_effective(), [m.astype(np.uint8) for m in sc.velocity_active]
+    r = ref_runner.run_reference_splat(sc.nx, sc.ny, sc.nz, sc.dx, P, vel, vact, apic=apic,
+                                       splat_bullet=splat_bullet)
+    payload = dict(shape=np.array([sc.nx, sc.ny, sc.nz], np.int32), dx=np.float64(sc.dx),
+                   apic=np.int32(apic), splat_bullet=np.int32(splat_bullet),
+                   particles=P.view(np.uint8).reshape(len(P), P.dtype.itemsize))
+    for d, k in enumerate("uvw"):
+        payload[k + "0"], payload[k + "0_active"] = vel[d], vact[d]
+        payload[k], payload[k + "_active"] = r["velocity"][d], r["velocity_active"][d]
+        payload[k + "_mass"], payload[k + "_momentum"] = r["mass"][d], r["momentum"][d]
+        payload[k + "_splat_active"] = r["splat_active"][d]
+    path = os.path.join(OUT, f"{name}.npz")
+    np.savez_compressed(path, **payload)
+    return path
+
+
 def main():
     if not ref_runner.ref_available("float"):
         raise SystemExit("compiled reference not found: run `make -C oracle/ref` first")
@@ -173,6 +203,11 @@ def main():
         if only and name not in only:
             continue
         p = make_extend(name, build)
+        print(p, os.path.getsize(p))
+    for name, build in SPLAT_CASES.items():
+        if only and name not in only:
+            continue
+        p = make_splat(name, build)
         print(p, os.path.getsize(p))
 
 
