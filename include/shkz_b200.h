@@ -197,6 +197,55 @@ int shkz_b200_extend_velocity_host(shkz_b200_ctx *ctx, const shkz_b200_extend_ar
  * 16-byte boundaries (cudaMalloc's are), else SHKZ_B200_ERR_ARG. */
 int shkz_b200_extend_velocity_device(shkz_b200_ctx *ctx, const shkz_b200_extend_args *args);
 
+/* FLIP splat before the projection: what the FLIP liquid solver does right
+ * before project() (macflipliquid3, src/liquid/macflipliquid3.cpp:135-151):
+ * macnbflip3::splat (src/flip/macnbflip3.cpp:103-148) -- every face within
+ * reach of a splatting particle gets the tent-weighted sums of particle mass
+ * and momentum (the APIC term c[d].(x_face - p) included), gathered over the
+ * particles' edge hash (pointgridhash3, src/pointgridhash/pointgridhash3.cpp:
+ * 90-100, 218-231) -- and then the combined grid velocity on every face with
+ * non-zero mass: u = (g u + momentum) / (g + mass), g = max(0, 1 - mass) on
+ * faces the velocity held active, else 0; the face becomes active.
+ * Results are bit-identical to the reference's.
+ *
+ * Particles are `count` records of `stride` bytes, read in place: a maintainer
+ * passes macnbflip3's own particle vector with stride sizeof(Particle) and the
+ * offsetof() of its fields. The float fields (p[3], velocity[3], mass,
+ * c[3][3]) must lie at offsets that are multiples of 4 with stride a multiple
+ * of 4; offset_apic = -1 turns APIC off (macnbflip3's APIC=No);
+ * offset_bullet = -1 means no bullet flags. Bullet particles splat only when
+ * splat_bullet != 0 (SplatBulletParticle). Face grids use the layouts of
+ * shkz_b200_project_args. mass, momentum and splat_active are optional outputs
+ * (all three or none): the splat grid itself, zero and inactive where the
+ * splatted mass is zero. nx, ny, nz >= 1; the three axes' edge grids together
+ * and 3 * count stay below 2^31. */
+typedef struct shkz_b200_splat_args {
+  int nx, ny, nz;
+  double dx;
+  long long count;                /* particles */
+  const void *particles;          /* count records of stride bytes */
+  int stride;
+  int offset_position;            /* float[3] */
+  int offset_velocity;            /* float[3] */
+  int offset_mass;                /* float */
+  int offset_apic;                /* float[3][3], row d = c[d]; -1: APIC off */
+  int offset_bullet;              /* uint8 (nonzero = bullet); -1: none */
+  int splat_bullet;
+  float *velocity[3];             /* faces, in/out */
+  uint8_t *velocity_active[3];    /* faces, in/out */
+  float *mass[3];                 /* faces, out, optional */
+  float *momentum[3];             /* faces, out, optional */
+  uint8_t *splat_active[3];       /* faces, out, optional */
+} shkz_b200_splat_args;
+
+/* Host buffers (particle records and grids copied to the device and back). */
+int shkz_b200_splat_host(shkz_b200_ctx *ctx, const shkz_b200_splat_args *args);
+
+/* Device pointers on the context's device (the particle records 4-byte
+ * aligned): the grid velocity can go straight on to
+ * shkz_b200_project_device. */
+int shkz_b200_splat_device(shkz_b200_ctx *ctx, const shkz_b200_splat_args *args);
+
 /* The CUDA stream the context launches on (as an opaque pointer), so callers
  * can order their own work against it. */
 void *shkz_b200_stream(shkz_b200_ctx *ctx);

@@ -31,6 +31,7 @@ UNITS = {
     "noalloc.cu": [],
     "warmstart.cu": [],
     "extend.cu": ["-fmad=false"],
+    "splat.cu": ["-fmad=false"],
 }
 HEADERS = ["common.cuh", "kernels.h", "solver.h", "learned.h", "tc_conv.cuh"]
 

@@ -92,6 +92,22 @@ struct shkz_b200_ctx {
   uint8_t *ext_a[3] = {};          // and its flags
   size_t cap_ext[3] = {0, 0, 0};
   int *ext_flag = nullptr;         // levelset_exist(solid) of the extension's constraint
+  // FLIP splat (splat.cu)
+  unsigned char *sp_raw = nullptr;  // particle records (host path)
+  size_t cap_sp_raw = 0;
+  float4 *sp_posm = nullptr, *sp_vc[3] = {};
+  int *sp_key = nullptr, *sp_rank = nullptr, *sp_list = nullptr;
+  float4 *sp_sposm = nullptr, *sp_svc = nullptr;
+  long long cap_sp_particles = 0;
+  int *sp_faces = nullptr, *sp_sorted = nullptr, *sp_face_bin = nullptr, *sp_nfaces = nullptr, *sp_work = nullptr;
+  long long cap_sp_list = 0;
+  int *sp_start = nullptr, *sp_tiles = nullptr;
+  long long cap_sp_buckets = 0;
+  uint8_t *sp_act[3] = {};
+  size_t cap_sp_faces[3] = {0, 0, 0};
+  float *sp_mass[3] = {}, *sp_mom[3] = {};  // optional outputs (host path)
+  uint8_t *sp_sact[3] = {};
+  size_t cap_sp_out[3] = {0, 0, 0};
   void *flush = nullptr;           // 256 MB written between timed kernel launches (> L2)
   size_t cap_h_dens[3] = {0, 0, 0};
 };
@@ -353,7 +369,12 @@ extern "C" void shkz_b200_destroy(shkz_b200_ctx *ctx) {
                   ctx->mtile, ctx->mnbr, ctx->msched, ctx->msub, ctx->mfaces_f, ctx->mfaces_b, ctx->curv,
                   ctx->prev, ctx->rank_pool, ctx->rank_cnt, ctx->rank_total, ctx->xw, ctx->h_dens[0],
                   ctx->h_dens[1], ctx->h_dens[2], ctx->flush, ctx->pb, ctx->ext_v[0], ctx->ext_v[1], ctx->ext_v[2],
-                  ctx->ext_a[0], ctx->ext_a[1], ctx->ext_a[2], ctx->ext_flag};
+                  ctx->ext_a[0], ctx->ext_a[1], ctx->ext_a[2], ctx->ext_flag, ctx->sp_raw, ctx->sp_posm,
+                  ctx->sp_vc[0], ctx->sp_vc[1], ctx->sp_vc[2], ctx->sp_key, ctx->sp_rank, ctx->sp_list, ctx->sp_sposm,
+                  ctx->sp_svc, ctx->sp_faces, ctx->sp_sorted, ctx->sp_face_bin, ctx->sp_nfaces, ctx->sp_work,
+                  ctx->sp_start, ctx->sp_tiles, ctx->sp_act[0], ctx->sp_act[1], ctx->sp_act[2], ctx->sp_mass[0],
+                  ctx->sp_mass[1], ctx->sp_mass[2], ctx->sp_mom[0], ctx->sp_mom[1], ctx->sp_mom[2],
+                  ctx->sp_sact[0], ctx->sp_sact[1], ctx->sp_sact[2]};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (ctx->model) learned_free(ctx->model);
@@ -1012,6 +1033,185 @@ extern "C" int shkz_b200_extend_velocity_host(shkz_b200_ctx *ctx, const shkz_b20
   for (int d = 0; d < 3; ++d) {
     SHKZ_CUDA_TRY(cudaMemcpyAsync(a->velocity[d], ctx->h_vel[d], nf[d] * 4, cudaMemcpyDeviceToHost, s));
     SHKZ_CUDA_TRY(cudaMemcpyAsync(a->velocity_active[d], ctx->h_vact[d], nf[d], cudaMemcpyDeviceToHost, s));
+  }
+  SHKZ_CUDA_TRY(cudaStreamSynchronize(s));
+  return 0;
+}
+
+// --------------------------------------------------------------------------
+// FLIP splat before the projection (macflipliquid3.cpp:135-151): kernels in
+// splat.cu.
+
+static long long splat_buckets(int nx, int ny, int nz, long long base[3]) {
+  long long total = 0;
+  for (int d = 0; d < 3; ++d) {
+    base[d] = total;
+    total += (long long)(nx + (d != 0)) * (ny + (d != 1)) * (nz + (d != 2));
+  }
+  return total;
+}
+
+static int validate_splat(const shkz_b200_splat_args *a) {
+  if (!a || a->nx < 1 || a->ny < 1 || a->nz < 1 || !(a->dx > 0.0) || a->count < 0) return SHKZ_B200_ERR_ARG;
+  if (a->nx > 65536 || a->ny > 65536 || a->nz > 65536) return SHKZ_B200_ERR_LIMIT;
+  long long base[3];
+  const long long buckets = splat_buckets(a->nx, a->ny, a->nz, base);
+  if (buckets + 1 >= ((long long)1 << 31) || 3 * a->count >= ((long long)1 << 31)) return SHKZ_B200_ERR_LIMIT;
+  for (int d = 0; d < 3; ++d)
+    if (!a->velocity[d] || !a->velocity_active[d]) return SHKZ_B200_ERR_ARG;
+  const bool out0 = a->mass[0] != nullptr;
+  for (int d = 0; d < 3; ++d)
+    if ((a->mass[d] != nullptr) != out0 || (a->momentum[d] != nullptr) != out0 ||
+        (a->splat_active[d] != nullptr) != out0)
+      return SHKZ_B200_ERR_ARG;
+  if (a->count == 0) return 0;
+  if (!a->particles || a->stride < 4 || (a->stride & 3)) return SHKZ_B200_ERR_ARG;
+  auto field = [&](int off, int bytes) { return off >= 0 && (off & 3) == 0 && off + bytes <= a->stride; };
+  if (!field(a->offset_position, 12) || !field(a->offset_velocity, 12) || !field(a->offset_mass, 4))
+    return SHKZ_B200_ERR_ARG;
+  if (a->offset_apic != -1 && !field(a->offset_apic, 36)) return SHKZ_B200_ERR_ARG;
+  if (a->offset_bullet != -1 && (a->offset_bullet < 0 || a->offset_bullet >= a->stride)) return SHKZ_B200_ERR_ARG;
+  return 0;
+}
+
+// particles: device records; grid: device face arrays (outputs optional)
+static int splat_device(shkz_b200_ctx *ctx, const shkz_b200_splat_args *a, const void *particles,
+                        const SplatGrid &grid) {
+  cudaStream_t s = ctx->stream;
+  SplatBuffers B{};
+  B.buckets = splat_buckets(a->nx, a->ny, a->nz, B.bucket_base);
+  B.apic = a->offset_apic >= 0;
+  const long long n = a->count;
+  if (n > ctx->cap_sp_particles) {
+    GROW(sp_posm, n);
+    for (int d = 0; d < 3; ++d) GROW(sp_vc[d], n);
+    GROW(sp_key, 3 * n);
+    GROW(sp_rank, 3 * n);
+    GROW(sp_list, 3 * n);
+    GROW(sp_sposm, 3 * n);
+    GROW(sp_svc, 3 * n);
+    ctx->cap_sp_particles = n;
+  }
+  if (!ctx->sp_nfaces) GROW(sp_nfaces, 3);
+  if (!ctx->sp_work) GROW(sp_work, 3 * kSplatWorkBins);
+  if (B.buckets + 1 > ctx->cap_sp_buckets) {
+    GROW(sp_start, B.buckets + 1);
+    GROW(sp_tiles, scan_tile_count(B.buckets + 1));
+    ctx->cap_sp_buckets = B.buckets + 1;
+  }
+  // a particle activates at most 8 faces per axis
+  size_t nf[3];
+  long long listed = 0;
+  for (int d = 0; d < 3; ++d) {
+    nf[d] = (size_t)(a->nx + (d == 0)) * (a->ny + (d == 1)) * (a->nz + (d == 2));
+    B.face_off[d] = listed;
+    listed += std::min((long long)nf[d], 8 * n);
+  }
+  if (listed > ctx->cap_sp_list) {
+    GROW(sp_faces, listed);
+    GROW(sp_sorted, listed);
+    GROW(sp_face_bin, listed);
+    ctx->cap_sp_list = listed;
+  }
+  for (int d = 0; d < 3; ++d) {
+    if (nf[d] > ctx->cap_sp_faces[d]) {
+      GROW(sp_act[d], nf[d]);
+      ctx->cap_sp_faces[d] = nf[d];
+    }
+    B.vc[d] = ctx->sp_vc[d];
+    B.act[d] = ctx->sp_act[d];
+    SHKZ_CUDA_TRY(cudaMemsetAsync(ctx->sp_act[d], 0, nf[d], s));
+  }
+  B.posm = ctx->sp_posm;
+  B.key = ctx->sp_key;
+  B.rank = ctx->sp_rank;
+  B.start = ctx->sp_start;
+  B.list = ctx->sp_list;
+  B.sposm = ctx->sp_sposm;
+  B.svc = ctx->sp_svc;
+  B.faces = ctx->sp_faces;
+  B.sorted = ctx->sp_sorted;
+  B.face_bin = ctx->sp_face_bin;
+  B.work = ctx->sp_work;
+  B.nfaces = ctx->sp_nfaces;
+  SHKZ_CUDA_TRY(cudaMemsetAsync(ctx->sp_start, 0, (size_t)(B.buckets + 1) * sizeof(int), s));
+  SHKZ_CUDA_TRY(cudaMemsetAsync(ctx->sp_nfaces, 0, 3 * sizeof(int), s));
+  SHKZ_CUDA_TRY(cudaMemsetAsync(ctx->sp_work, 0, 3 * kSplatWorkBins * sizeof(int), s));
+  SplatRecords R{static_cast<const unsigned char *>(particles), n, a->stride, a->offset_position,
+                 a->offset_velocity, a->offset_mass, a->offset_apic, a->offset_bullet, a->splat_bullet != 0};
+  launch_splat_bin(R, a->nx, a->ny, a->nz, a->dx, B, s);
+  launch_exclusive_scan(ctx->sp_start, B.buckets + 1, ctx->sp_tiles, s);
+  launch_splat_scatter(n, B, s);
+  launch_splat_gather(a->nx, a->ny, a->nz, a->dx, B, grid, s);
+  SHKZ_CUDA_TRY(cudaGetLastError());
+  SHKZ_CUDA_TRY(cudaStreamSynchronize(s));
+  return 0;
+}
+
+extern "C" int shkz_b200_splat_device(shkz_b200_ctx *ctx, const shkz_b200_splat_args *a) {
+  if (!ctx) return SHKZ_B200_ERR_ARG;
+  int rc = validate_splat(a);
+  if (rc) return rc;
+  if (a->count && ((uintptr_t)a->particles & 3u)) return SHKZ_B200_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  SplatGrid G{};
+  for (int d = 0; d < 3; ++d) {
+    G.velocity[d] = a->velocity[d];
+    G.velocity_active[d] = a->velocity_active[d];
+    G.mass[d] = a->mass[d];
+    G.momentum[d] = a->momentum[d];
+    G.splat_active[d] = a->splat_active[d];
+  }
+  return splat_device(ctx, a, a->particles, G);
+}
+
+extern "C" int shkz_b200_splat_host(shkz_b200_ctx *ctx, const shkz_b200_splat_args *a) {
+  if (!ctx) return SHKZ_B200_ERR_ARG;
+  int rc = validate_splat(a);
+  if (rc) return rc;
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  const Geometry G = make_geometry(a->nx, a->ny, a->nz);
+  const bool svel[3] = {false, false, false};
+  rc = ensure_host_staging(ctx, G, false, svel);
+  if (rc) return rc;
+  const size_t raw = (size_t)a->count * (size_t)(a->count ? a->stride : 0);
+  if (raw > ctx->cap_sp_raw) {
+    GROW(sp_raw, raw);
+    ctx->cap_sp_raw = raw;
+  }
+  if (raw) SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->sp_raw, a->particles, raw, cudaMemcpyHostToDevice, s));
+  const bool outs = a->mass[0] != nullptr;
+  SplatGrid D{};
+  size_t nf[3];
+  for (int d = 0; d < 3; ++d) {
+    nf[d] = (size_t)(a->nx + (d == 0)) * (a->ny + (d == 1)) * (a->nz + (d == 2));
+    SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->h_vel[d], a->velocity[d], nf[d] * 4, cudaMemcpyHostToDevice, s));
+    SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->h_vact[d], a->velocity_active[d], nf[d], cudaMemcpyHostToDevice, s));
+    D.velocity[d] = ctx->h_vel[d];
+    D.velocity_active[d] = ctx->h_vact[d];
+    if (outs) {
+      if (nf[d] > ctx->cap_sp_out[d]) {
+        GROW(sp_mass[d], nf[d]);
+        GROW(sp_mom[d], nf[d]);
+        GROW(sp_sact[d], nf[d]);
+        ctx->cap_sp_out[d] = nf[d];
+      }
+      D.mass[d] = ctx->sp_mass[d];
+      D.momentum[d] = ctx->sp_mom[d];
+      D.splat_active[d] = ctx->sp_sact[d];
+    }
+  }
+  rc = splat_device(ctx, a, ctx->sp_raw, D);
+  if (rc) return rc;
+  for (int d = 0; d < 3; ++d) {
+    SHKZ_CUDA_TRY(cudaMemcpyAsync(a->velocity[d], ctx->h_vel[d], nf[d] * 4, cudaMemcpyDeviceToHost, s));
+    SHKZ_CUDA_TRY(cudaMemcpyAsync(a->velocity_active[d], ctx->h_vact[d], nf[d], cudaMemcpyDeviceToHost, s));
+    if (outs) {
+      SHKZ_CUDA_TRY(cudaMemcpyAsync(a->mass[d], ctx->sp_mass[d], nf[d] * 4, cudaMemcpyDeviceToHost, s));
+      SHKZ_CUDA_TRY(cudaMemcpyAsync(a->momentum[d], ctx->sp_mom[d], nf[d] * 4, cudaMemcpyDeviceToHost, s));
+      SHKZ_CUDA_TRY(cudaMemcpyAsync(a->splat_active[d], ctx->sp_sact[d], nf[d], cudaMemcpyDeviceToHost, s));
+    }
   }
   SHKZ_CUDA_TRY(cudaStreamSynchronize(s));
   return 0;

@@ -59,6 +59,49 @@ void launch_solid_exists(const float *solid, const uint8_t *act, size_t n, int *
 void launch_constrain_find(int d, int nx, int ny, int nz, double dx, const float *solid, const int *solid_flag,
                            const ConstrainFields &f, float *side, uint8_t *flag, cudaStream_t s);
 void launch_apply_side(size_t n, float *v, const float *side, uint8_t *flag, cudaStream_t s);
+
+// FLIP splat (splat.cu). Particle records read in place: float fields at byte
+// offsets (multiples of 4) of `stride`-byte records.
+constexpr int kSplatWorkBins = 64;  // work classes of 4 particle visits each
+struct SplatRecords {
+  const unsigned char *base;
+  long long count;
+  int stride, off_p, off_v, off_m, off_c, off_bullet;  // off_c / off_bullet < 0: absent
+  int splat_bullet;
+};
+struct SplatBuffers {
+  float4 *posm;            // per particle: p, mass
+  float4 *vc[3];           // per particle and axis d: u_d, c[d]
+  int *key, *rank;         // [3][count]: global edge bucket (-1: does not splat), slot in it
+  int *start;              // buckets + 1 counters, scanned into bucket starts
+  int *list;               // [3 count] particle indices, bucket by bucket, arrival order inside one
+  float4 *sposm, *svc;     // [3 count] posm and vc[d] bucket by bucket, index order inside one
+  uint8_t *act[3];         // faces activated by the splat
+  int *faces;              // active faces of each axis, listed from face_off[d]
+  int *sorted;             // the same lists, faces with more particles to visit first
+  int *face_bin;           // work class of each listed face
+  int *work;               // [3][kSplatWorkBins] work-class counts, then cursors
+  int *nfaces;             // [3] list lengths
+  long long face_off[3];
+  long long bucket_base[3];
+  long long buckets;
+  int apic;
+};
+struct SplatGrid {
+  float *velocity[3];
+  uint8_t *velocity_active[3];
+  float *mass[3], *momentum[3];  // optional (mass[0] == nullptr: none)
+  uint8_t *splat_active[3];
+};
+void launch_splat_bin(const SplatRecords &R, int nx, int ny, int nz, double dx, const SplatBuffers &B,
+                      cudaStream_t s);
+size_t scan_tile_count(long long n);
+void launch_exclusive_scan(int *data, long long n, int *tile_sums, cudaStream_t s);
+// bucket lists, then the particles' data copied into bucket order
+void launch_splat_scatter(long long count, const SplatBuffers &B, cudaStream_t s);
+// active-face lists ordered by work, then the per-face sums and the combined velocity
+void launch_splat_gather(int nx, int ny, int nz, double dx, const SplatBuffers &B, const SplatGrid &G,
+                         cudaStream_t s);
 void launch_surface_tension(const AssemblyInputs &in, const int *flags, float *curv, double kappa, float *const vel[3],
                             const uint8_t *const vact[3], cudaStream_t s);
 void launch_scatter_pressure(const Geometry &G, const int *tile_state, const float *pressure_pool, const uint8_t *unk,

@@ -71,6 +71,17 @@ class ExtendArgs(ctypes.Structure):
     ]
 
 
+class SplatArgs(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("dx", ctypes.c_double),
+        ("count", ctypes.c_longlong), ("particles", ctypes.c_void_p), ("stride", ctypes.c_int),
+        ("offset_position", ctypes.c_int), ("offset_velocity", ctypes.c_int), ("offset_mass", ctypes.c_int),
+        ("offset_apic", ctypes.c_int), ("offset_bullet", ctypes.c_int), ("splat_bullet", ctypes.c_int),
+        ("velocity", ctypes.c_void_p * 3), ("velocity_active", ctypes.c_void_p * 3),
+        ("mass", ctypes.c_void_p * 3), ("momentum", ctypes.c_void_p * 3), ("splat_active", ctypes.c_void_p * 3),
+    ]
+
+
 class Result(ctypes.Structure):
     _fields_ = [
         ("status", ctypes.c_int), ("iterations", ctypes.c_int), ("outer_steps", ctypes.c_int),
@@ -98,6 +109,7 @@ EXPORTS = [
     "shkz_b200_set_target_volume", "shkz_b200_get_volume_state", "shkz_b200_set_volume_state",
     "shkz_b200_warm_start_size", "shkz_b200_get_warm_start", "shkz_b200_set_warm_start",
     "shkz_b200_learned_flops", "shkz_b200_extend_velocity_host", "shkz_b200_extend_velocity_device",
+    "shkz_b200_splat_host", "shkz_b200_splat_device",
 ]
 
 _lib = None
@@ -125,6 +137,8 @@ def load(path: str = LIB_PATH):
     L.shkz_b200_project_device.argtypes = [P, ctypes.POINTER(ProjectArgs), ctypes.POINTER(Result)]
     L.shkz_b200_extend_velocity_host.argtypes = [P, ctypes.POINTER(ExtendArgs)]
     L.shkz_b200_extend_velocity_device.argtypes = [P, ctypes.POINTER(ExtendArgs)]
+    L.shkz_b200_splat_host.argtypes = [P, ctypes.POINTER(SplatArgs)]
+    L.shkz_b200_splat_device.argtypes = [P, ctypes.POINTER(SplatArgs)]
     L.shkz_b200_stream.argtypes = [P]
     L.shkz_b200_stream.restype = P
     L.shkz_b200_solve_csr.argtypes = [P, ctypes.c_longlong, P, P, P, P, P, ctypes.POINTER(Result)]
@@ -238,3 +252,46 @@ def extend_velocity(ctx: Context, velocity, velocity_active, solid, solid_active
         a.velocity_active[d] = act[d].ctypes.data
     ctx.check(load().shkz_b200_extend_velocity_host(ctx.handle, ctypes.byref(a)), "shkz_b200_extend_velocity_host")
     return vel, act
+
+
+def splat_args(nx: int, ny: int, nz: int, dx: float, particles, count: int, record_dtype, apic: bool = True,
+               splat_bullet: bool = False) -> SplatArgs:
+    """shkz_b200_splat_args for particle records of a numpy structured dtype
+    with fields p, velocity, mass, c and bullet (the reference's layout is
+    ``shiokaze_b200.scenes.PARTICLE_DTYPE``) at address ``particles``; the
+    grid pointers are left for the caller."""
+    a = SplatArgs()
+    a.nx, a.ny, a.nz, a.dx = nx, ny, nz, float(dx)
+    a.count, a.particles, a.stride = int(count), particles, record_dtype.itemsize
+    off = lambda k: record_dtype.fields[k][1]
+    a.offset_position, a.offset_velocity, a.offset_mass = off("p"), off("velocity"), off("mass")
+    a.offset_apic = off("c") if apic else -1
+    a.offset_bullet = off("bullet") if "bullet" in record_dtype.fields else -1
+    a.splat_bullet = int(bool(splat_bullet))
+    return a
+
+
+def splat(ctx: Context, nx: int, ny: int, nz: int, dx: float, particles, velocity, velocity_active,
+          apic: bool = True, splat_bullet: bool = False, outputs: bool = True):
+    """The FLIP splat and combined grid velocity the FLIP liquid solver runs
+    right before a projection (macflipliquid3.cpp:135-151), on host numpy data
+    through ``shkz_b200_splat_host``. ``particles`` is a structured array of
+    particle records. Returns (velocity, velocity_active, mass, momentum,
+    splat_active), lists of three face grids (the last three None without
+    ``outputs``)."""
+    import numpy as np
+    P = np.ascontiguousarray(particles)
+    vel = [np.ascontiguousarray(v, np.float32).copy() for v in velocity]
+    act = [np.ascontiguousarray(m, np.uint8).copy() for m in velocity_active]
+    a = splat_args(nx, ny, nz, dx, P.ctypes.data if len(P) else None, len(P), P.dtype, apic, splat_bullet)
+    mass = mom = sact = None
+    if outputs:
+        mass = [np.zeros_like(v) for v in vel]
+        mom = [np.zeros_like(v) for v in vel]
+        sact = [np.zeros_like(m) for m in act]
+    for d in range(3):
+        a.velocity[d], a.velocity_active[d] = vel[d].ctypes.data, act[d].ctypes.data
+        if outputs:
+            a.mass[d], a.momentum[d], a.splat_active[d] = mass[d].ctypes.data, mom[d].ctypes.data, sact[d].ctypes.data
+    ctx.check(load().shkz_b200_splat_host(ctx.handle, ctypes.byref(a)), "shkz_b200_splat_host")
+    return vel, act, mass, mom, sact

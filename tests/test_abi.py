@@ -42,3 +42,31 @@ def test_library_is_sm100a_only():
 def test_python_binding_lists_every_export():
     from shiokaze_b200 import native
     assert set(native.EXPORTS) == set(declared_functions())
+
+
+def test_ctypes_structs_match_the_header(tmp_path):
+    """Every argument struct of the C ABI has the same size and field offsets
+    in the header (compiled here with the system C compiler) as in the
+    Python binding."""
+    import subprocess
+    from shiokaze_b200 import native
+    structs = {"shkz_b200_config": native.Config, "shkz_b200_project_args": native.ProjectArgs,
+               "shkz_b200_result": native.Result, "shkz_b200_extend_args": native.ExtendArgs,
+               "shkz_b200_splat_args": native.SplatArgs}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "shkz_b200.h"', 'int main(void) {']
+    for cname, py in structs.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for field, _ in py._fields_:
+            lines.append(f'printf("{cname} {field} %zu\\n", offsetof({cname}, {field}));')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    include = os.path.join(ROOT, "include")
+    subprocess.check_call(["gcc", "-I", include, str(src), "-o", str(exe)])
+    out = subprocess.check_output([str(exe)], text=True).split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l}
+    for cname, py in structs.items():
+        assert got[(cname, "size")] == ctypes.sizeof(py), cname
+        for field, _ in py._fields_:
+            assert got[(cname, field)] == getattr(py, field).offset, (cname, field)
