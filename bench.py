@@ -58,6 +58,16 @@ ALGO_BYTES = {
 # One fused MIC(0)-PCG iteration: stencil pass 32 + sweep pair 72.
 ITER_BYTES = 104
 
+# FLIP splat workload (--workload flip_splat): the splat and combined grid
+# velocity before a projection, on the 256^3 sloshing tank with particles in
+# the 3-cell narrow band at 8 per cell. Algorithmic bytes: every particle's
+# record fields read once (p 12, c 36, velocity 12, mass 4, bullet 1) and
+# every splatted face's velocity and mask read and written (4 + 1 + 4 + 1).
+SPLAT_METRIC = "ms/splat (FLIP splat + combined grid velocity) at 256³, 3-cell narrow band, 8 particles/cell"
+SPLAT_UNIT = "ms/splat"
+SPLAT_BYTES_PARTICLE = 65
+SPLAT_BYTES_FACE = 10
+
 
 def job_ms_per_projection(elapsed_ms: float, steps: int, world: int, device=None) -> float:
     """Whole-job ms per projection: the slowest rank's timed region (max over
@@ -179,6 +189,185 @@ def cpu_reference_sample(n: int = 128):
                       f"{o.iterations} iterations, 1 projection"}
 
 
+def splat_workload(n: int):
+    from shiokaze_b200 import scenes
+    sc = scenes.sloshing_tank(n=n, seed=0, tol=1e-6)
+    P = scenes.flip_particles(sc, per_cell=8, seed=0, band=3.0)
+    return sc, P
+
+
+def splat_reference_sample(n: int):
+    """The compiled reference splat (oracle/_ref shkz_ref_splat: pointgridhash3
+    hash, macnbflip3::splat, combined velocity) on the splat workload at n^3;
+    its own timers, file I/O excluded."""
+    from oracle import ref_runner
+    sc, P = splat_workload(n)
+    r = ref_runner.run_reference_splat(sc.nx, sc.ny, sc.nz, sc.dx, P, sc.velocity_effective(),
+                                       [m.astype(np.uint8) for m in sc.velocity_active])
+    return sc, P, r["hash_ms"] + r["splat_ms"] + r["combine_ms"]
+
+
+def run_splat_reference_arm(args):
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    from oracle import ref_runner
+    if not ref_runner.ref_available("float"):
+        print(json.dumps({"impl": "reference", "unavailable": "compiled reference splat (oracle/_ref) not built"}))
+        return 0
+    budget_s = float(os.environ.get("SHKZ_REF_BUDGET_S", "240"))
+    times, t_start = [], time.perf_counter()
+    while len(times) < max(1, args.steps):
+        sc, P, ms = splat_reference_sample(args.n)
+        times.append(ms)
+        if time.perf_counter() - t_start > budget_s:
+            break
+    value = float(np.mean(times))
+    sample = (f"sloshing tank {args.n}^3, {len(P)} particles, reference pointgridhash3 + macnbflip3::splat + "
+              f"combined velocity, {len(times)} of {args.steps} requested splats within {budget_s:.0f} s")
+    line = {"metric": SPLAT_METRIC, "value": value, "unit": SPLAT_UNIT, "n_gpus": args.gpus, "steps": len(times),
+            "warmup": 0, "ms_per_step": value, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 weights into f32 sums", "data": "synthetic", "impl": "reference",
+            "config": {"workload": f"flip_splat sloshing_tank {args.n}^3, 3-cell band, 8 particles/cell, APIC"},
+            "cpu_baseline": {"value": value, "unit": SPLAT_UNIT, "cores": os.cpu_count(), "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": SPLAT_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_splat(args):
+    """The FLIP splat workload on the device: particles and grids resident in
+    HBM; a step restores the input velocity (device copy) and runs
+    shkz_b200_splat_device. e2e: shkz_b200_splat_host with pinned host arrays."""
+    import torch
+    import torch.distributed as dist
+    from shiokaze_b200 import native
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    sc, P = splat_workload(args.n)
+    nx, ny, nz = sc.nx, sc.ny, sc.nz
+    cfg = native.default_config()
+    cfg.device = local
+    ctx = native.Context(cfg)
+    L = native.load()
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    T = lambda arr: torch.from_numpy(np.ascontiguousarray(arr)).to(dev)
+    rec = T(P.view(np.uint8))
+    vel0 = [T(v) for v in sc.velocity_effective()]
+    act0 = [T(m.astype(np.uint8)) for m in sc.velocity_active]
+    vel = [v.clone() for v in vel0]
+    act = [m.clone() for m in act0]
+    sact = [torch.zeros_like(m) for m in act0]
+    mass = [torch.zeros_like(v) for v in vel0]
+    mom = [torch.zeros_like(v) for v in vel0]
+    torch.cuda.synchronize(dev)
+    a = native.splat_args(nx, ny, nz, sc.dx, rec.data_ptr(), len(P), P.dtype, apic=True)
+    for d in range(3):
+        a.velocity[d], a.velocity_active[d] = vel[d].data_ptr(), act[d].data_ptr()
+
+    def step():
+        with torch.cuda.stream(stream):
+            for d in range(3):
+                vel[d].copy_(vel0[d], non_blocking=True)
+                act[d].copy_(act0[d], non_blocking=True)
+        ctx.check(L.shkz_b200_splat_device(ctx.handle, ctypes.byref(a)), "shkz_b200_splat_device")
+
+    # untimed: the splat grid, for the count of splatted faces
+    b = native.splat_args(nx, ny, nz, sc.dx, rec.data_ptr(), len(P), P.dtype, apic=True)
+    for d in range(3):
+        b.velocity[d], b.velocity_active[d] = vel[d].data_ptr(), act[d].data_ptr()
+        b.mass[d], b.momentum[d], b.splat_active[d] = mass[d].data_ptr(), mom[d].data_ptr(), sact[d].data_ptr()
+    ctx.check(L.shkz_b200_splat_device(ctx.handle, ctypes.byref(b)), "shkz_b200_splat_device")
+    faces = int(sum(int(x.sum()) for x in sact))
+    for _ in range(args.warmup):
+        step()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    value = job_ms_per_projection(ev0.elapsed_time(ev1), args.steps, world, dev)
+    # the splat call alone (no restore copies) for the roofline
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        ctx.check(L.shkz_b200_splat_device(ctx.handle, ctypes.byref(a)), "shkz_b200_splat_device")
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    call_ms = e0.elapsed_time(e1) / args.steps
+    algo = SPLAT_BYTES_PARTICLE * len(P) + SPLAT_BYTES_FACE * faces
+    peak, peak_kind = measured_peaks()
+    achieved = algo / (call_ms * 1e-3) / 1e9
+    roofline = {"kernel": "shkz_b200_splat_device (bin, scan, bucket sort, face lists, k_splat_gather x3)",
+                "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_kind": peak_kind, "ms": call_ms, "algo_bytes_per_launch": algo, "traffic": None,
+                "note": ("not HBM-bound: the gather (about 3/4 of the call) is bound by FP64 issue and lane "
+                         "divergence, each face summing its particles serially in the reference's order")}
+    # end to end through the host-buffer entry point, pinned host arrays
+    pin = lambda arr: torch.from_numpy(np.ascontiguousarray(arr)).pin_memory()
+    h_rec = pin(P.view(np.uint8))
+    h_vel0 = [v.copy() for v in sc.velocity_effective()]
+    h_act0 = [m.astype(np.uint8) for m in sc.velocity_active]
+    h_vel = [pin(v) for v in h_vel0]
+    h_act = [pin(m) for m in h_act0]
+    ha = native.splat_args(nx, ny, nz, sc.dx, h_rec.data_ptr(), len(P), P.dtype, apic=True)
+    for d in range(3):
+        ha.velocity[d], ha.velocity_active[d] = h_vel[d].data_ptr(), h_act[d].data_ptr()
+    tot = 0.0
+    for i in range(args.steps + 1):
+        for d in range(3):
+            h_vel[d].numpy()[...] = h_vel0[d]
+            h_act[d].numpy()[...] = h_act0[d]
+        t0 = time.perf_counter()
+        ctx.check(L.shkz_b200_splat_host(ctx.handle, ctypes.byref(ha)), "shkz_b200_splat_host")
+        if i > 0:
+            tot += (time.perf_counter() - t0) * 1e3
+    nfaces = sum(v.numel() for v in h_vel)
+    e2e = {"value": tot / args.steps, "unit": SPLAT_UNIT, "h2d_bytes_per_step": int(h_rec.numel() + 5 * nfaces),
+           "d2h_bytes_per_step": int(5 * nfaces), "steps": args.steps, "timer": "host wall clock around the call"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            from oracle import ref_runner
+            if ref_runner.ref_available("float"):
+                _, Ps, ms = splat_reference_sample(128)
+                cpu = {"value": ms, "unit": SPLAT_UNIT, "cores": os.cpu_count(), "kind": "reference",
+                       "sample": f"sloshing tank 128^3 (1/8 of the cells), {len(Ps)} particles: reference "
+                                 f"pointgridhash3 hash + macnbflip3::splat + combined velocity, its own timers"}
+        except Exception as exc:
+            cpu = {"error": str(exc)}
+    if rank == 0:
+        line = {"metric": SPLAT_METRIC, "value": value, "unit": SPLAT_UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": value, "higher_is_better": False, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64 weights into f32 sums", "data": "synthetic",
+                "config": {"workload": f"flip_splat sloshing_tank {nx}^3, 3-cell band, 8 particles/cell, APIC",
+                           "particles": len(P), "splatted_faces": faces,
+                           "l2": "particle records 0.2 GB + face grids 0.25 GB > 126 MB L2 (no flush needed)",
+                           "step": "device velocity restore + one splat"},
+                "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(),
+                "gpu_launches": args.steps * 19}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -240,7 +429,14 @@ def main():
                     help="sloshing_tank 256^3 (headline), splash 384^3, dambreak_rain 512^3, dambreak_sphere 64^3")
     ap.add_argument("--learned-steps", type=int, default=2,
                     help="timed projections of the learned-preconditioner arm (0: skip)")
+    ap.add_argument("--workload", default="projection", choices=["projection", "flip_splat"],
+                    help="projection (headline) or the FLIP splat before it")
     args = ap.parse_args()
+    if args.workload == "flip_splat":
+        if args.impl == "reference":
+            return run_splat_reference_arm(args)
+        args.warmup = max(args.warmup, 3)
+        return run_splat(args)
     if args.impl == "reference":
         return run_reference_arm(args)
     args.warmup = max(args.warmup, 3)

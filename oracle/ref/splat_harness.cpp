@@ -11,6 +11,8 @@
 // every face the splat left active, which then becomes active).
 //
 // usage: shkz_ref_splat <in.bin> <out.bin> [Key=Value ...]
+//   prints "hash_ms H splat_ms S combine_ms C": wall time of the particle
+//   hash (sort_particles), the splat and the combined velocity
 //   configuration keys go to the reference (APIC=Yes|No,
 //   SplatBulletParticle=Yes|No, ...)
 //
@@ -27,6 +29,7 @@
 #include <shiokaze/array/macarray3.h>
 #include <shiokaze/core/configuration.h>
 #include <shiokaze/core/credit.h>
+#include <chrono>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -119,7 +122,9 @@ int main( int argc, const char *argv[] ) {
 		q.r = 0.25*dx;
 		q.bullet = bullet[n];
 	}
+	const auto t0 = std::chrono::steady_clock::now();
 	root.m_flip.load_particles(particles);
+	const auto t1 = std::chrono::steady_clock::now();
 	//
 	auto &velocity = root.m_velocity;
 	velocity.initialize(shape);
@@ -138,7 +143,9 @@ int main( int argc, const char *argv[] ) {
 	//
 	auto &mm = root.m_mass_momentum;
 	mm.initialize(shape);
+	const auto t2 = std::chrono::steady_clock::now();
 	root.m_flip.run_splat(time,mm);
+	const auto t3 = std::chrono::steady_clock::now();
 	//
 	// combined grid velocity: every value is computed from the velocity
 	// before any is written, then all are written
@@ -159,6 +166,9 @@ int main( int argc, const char *argv[] ) {
 			velocity[dim].set(i,j,k,combined[dim][i+(size_t)fs.w*(j+(size_t)fs.h*k)]);
 		});
 	}
+	const auto t4 = std::chrono::steady_clock::now();
+	auto ms = []( auto a, auto b ) { return std::chrono::duration<double,std::milli>(b-a).count(); };
+	std::printf("hash_ms %.6f splat_ms %.6f combine_ms %.6f\n",ms(t0,t1),ms(t2,t3),ms(t3,t4));
 	//
 	FILE *out = std::fopen(argv[2],"wb");
 	if( ! out ) { std::fprintf(stderr,"cannot write %s\n",argv[2]); return 2; }

@@ -128,7 +128,8 @@ def run_reference_splat(nx: int, ny: int, nz: int, dx: float, particles: np.ndar
     """Run the compiled reference FLIP splat (``shkz_ref_splat``: macnbflip3::splat
     then the combined grid velocity of macflipliquid3) on particle records in
     the reference's layout. Returns face grids (lists over dim) under
-    ``mass``, ``momentum``, ``splat_active``, ``velocity``, ``velocity_active``."""
+    ``mass``, ``momentum``, ``splat_active``, ``velocity``, ``velocity_active``,
+    and the reference's wall times ``hash_ms``, ``splat_ms``, ``combine_ms``."""
     exe = os.path.join(REF_DIR, variant, "shkz_ref_splat")
     P = np.ascontiguousarray(particles)
     n = len(P)
@@ -153,6 +154,9 @@ def run_reference_splat(nx: int, ny: int, nz: int, dx: float, particles: np.ndar
         if proc.returncode != 0:
             raise RuntimeError(f"reference splat failed ({proc.returncode}):\n{proc.stdout[-2000:]}\n{proc.stderr[-2000:]}")
         out = {k: [] for k in ("mass", "momentum", "splat_active", "velocity", "velocity_active")}
+        m = re.search(r"hash_ms ([0-9.]+) splat_ms ([0-9.]+) combine_ms ([0-9.]+)", proc.stdout)
+        if m:
+            out["hash_ms"], out["splat_ms"], out["combine_ms"] = (float(x) for x in m.groups())
         with open(fout, "rb") as f:
             for d in range(3):
                 shp = (nz + (d == 2), ny + (d == 1), nx + (d == 0))

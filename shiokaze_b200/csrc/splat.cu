@@ -364,14 +364,30 @@ __global__ void k_splat_work_scan(SplatBuffers B) {
   }
 }
 
+// Faces into class order. A block counts its faces per class in shared
+// memory, reserves each class's run in one global atomic, and places its
+// faces with shared-memory cursors (the global cursors would serialise on a
+// few addresses).
 template <int D>
 __global__ void __launch_bounds__(256) k_splat_face_sort(SplatBuffers B) {
+  __shared__ int cnt[kSplatWorkBins];
+  __shared__ int cur[kSplatWorkBins];
   const int nact = B.nfaces[D];
   const int *faces = B.faces + B.face_off[D];
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nact; t += gridDim.x * blockDim.x) {
-    const int bin = B.face_bin[B.face_off[D] + t];
-    const int at = atomicAdd(&B.work[D * kSplatWorkBins + bin], 1);
-    B.sorted[B.face_off[D] + at] = faces[t];
+  const int *bins = B.face_bin + B.face_off[D];
+  const int stride = gridDim.x * blockDim.x;
+  for (int c0 = blockIdx.x * blockDim.x; c0 < nact; c0 += stride) {
+    for (int i = threadIdx.x; i < kSplatWorkBins; i += blockDim.x) cnt[i] = 0;
+    __syncthreads();
+    const int t = c0 + threadIdx.x;
+    const int bin = t < nact ? bins[t] : -1;
+    if (bin >= 0) atomicAdd(&cnt[bin], 1);
+    __syncthreads();
+    for (int i = threadIdx.x; i < kSplatWorkBins; i += blockDim.x)
+      cur[i] = cnt[i] ? atomicAdd(&B.work[D * kSplatWorkBins + i], cnt[i]) : 0;
+    __syncthreads();
+    if (bin >= 0) B.sorted[B.face_off[D] + atomicAdd(&cur[bin], 1)] = faces[t];
+    __syncthreads();
   }
 }
 
