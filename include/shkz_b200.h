@@ -218,7 +218,10 @@ int shkz_b200_extend_velocity_device(shkz_b200_ctx *ctx, const shkz_b200_extend_
  * shkz_b200_project_args. mass, momentum and splat_active are optional outputs
  * (all three or none): the splat grid itself, zero and inactive where the
  * splatted mass is zero. nx, ny, nz >= 1; the three axes' edge grids together
- * and 3 * count stay below 2^31. */
+ * and 3 * count stay below 2^31. An edge bucket (the particles whose
+ * positions round to one edge cell; about 8 to 12 in a FLIP simulation) of
+ * more than 4096 particles returns SHKZ_B200_ERR_LIMIT with the grids left
+ * as they were. */
 typedef struct shkz_b200_splat_args {
   int nx, ny, nz;
   double dx;

@@ -1092,7 +1092,7 @@ static int splat_device(shkz_b200_ctx *ctx, const shkz_b200_splat_args *a, const
     GROW(sp_svc, 3 * n);
     ctx->cap_sp_particles = n;
   }
-  if (!ctx->sp_nfaces) GROW(sp_nfaces, 3);
+  if (!ctx->sp_nfaces) GROW(sp_nfaces, 4);
   if (!ctx->sp_work) GROW(sp_work, 3 * kSplatWorkBins);
   if (B.buckets + 1 > ctx->cap_sp_buckets) {
     GROW(sp_start, B.buckets + 1);
@@ -1135,7 +1135,7 @@ static int splat_device(shkz_b200_ctx *ctx, const shkz_b200_splat_args *a, const
   B.work = ctx->sp_work;
   B.nfaces = ctx->sp_nfaces;
   SHKZ_CUDA_TRY(cudaMemsetAsync(ctx->sp_start, 0, (size_t)(B.buckets + 1) * sizeof(int), s));
-  SHKZ_CUDA_TRY(cudaMemsetAsync(ctx->sp_nfaces, 0, 3 * sizeof(int), s));
+  SHKZ_CUDA_TRY(cudaMemsetAsync(ctx->sp_nfaces, 0, 4 * sizeof(int), s));
   SHKZ_CUDA_TRY(cudaMemsetAsync(ctx->sp_work, 0, 3 * kSplatWorkBins * sizeof(int), s));
   SplatRecords R{static_cast<const unsigned char *>(particles), n, a->stride, a->offset_position,
                  a->offset_velocity, a->offset_mass, a->offset_apic, a->offset_bullet, a->splat_bullet != 0};
@@ -1144,8 +1144,10 @@ static int splat_device(shkz_b200_ctx *ctx, const shkz_b200_splat_args *a, const
   launch_splat_scatter(n, B, s);
   launch_splat_gather(a->nx, a->ny, a->nz, a->dx, B, grid, s);
   SHKZ_CUDA_TRY(cudaGetLastError());
+  int over = 0;
+  SHKZ_CUDA_TRY(cudaMemcpyAsync(&over, ctx->sp_nfaces + 3, sizeof(int), cudaMemcpyDeviceToHost, s));
   SHKZ_CUDA_TRY(cudaStreamSynchronize(s));
-  return 0;
+  return over ? SHKZ_B200_ERR_LIMIT : 0;
 }
 
 extern "C" int shkz_b200_splat_device(shkz_b200_ctx *ctx, const shkz_b200_splat_args *a) {

@@ -63,6 +63,9 @@ void launch_apply_side(size_t n, float *v, const float *side, uint8_t *flag, cud
 // FLIP splat (splat.cu). Particle records read in place: float fields at byte
 // offsets (multiples of 4) of `stride`-byte records.
 constexpr int kSplatWorkBins = 64;  // work classes of 4 particle visits each
+// Largest edge bucket the splat accepts (particles of one edge cell, about 8
+// to 12 in a FLIP simulation): ordering a bucket costs its size squared.
+constexpr int kSplatBucketLimit = 4096;
 struct SplatRecords {
   const unsigned char *base;
   long long count;
@@ -81,7 +84,7 @@ struct SplatBuffers {
   int *sorted;             // the same lists, faces with more particles to visit first
   int *face_bin;           // work class of each listed face
   int *work;               // [3][kSplatWorkBins] work-class counts, then cursors
-  int *nfaces;             // [3] list lengths
+  int *nfaces;             // [4]: list lengths of the three axes, then a bucket over kSplatBucketLimit (flag)
   long long face_off[3];
   long long bucket_base[3];
   long long buckets;

@@ -256,6 +256,11 @@ __global__ void k_splat_sort_copy(long long count, SplatBuffers B) {
   const int n = B.list[s];
   const int key = B.key[(size_t)d * count + n];
   const int s0 = B.start[key], s1 = B.start[key + 1];
+  if (s1 - s0 > kSplatBucketLimit) {
+    // refused (the call returns SHKZ_B200_ERR_LIMIT and the gather writes nothing)
+    if (s == s0) B.nfaces[3] = 1;
+    return;
+  }
   int r = 0;
   for (int t = s0; t < s1; ++t) r += B.list[t] < n;
   B.sposm[s0 + r] = B.posm[n];
@@ -412,6 +417,7 @@ template <int D, bool POW2>
 __global__ void __launch_bounds__(kGatherThreads) k_splat_gather(int nx, int ny, int nz, DxDiv X, SplatBuffers B,
                                                                  SplatGrid G) {
   __shared__ int2 range[8][kGatherThreads];
+  if (B.nfaces[3]) return;  // a bucket was over the limit: leave the grids as they are
   const int fw = nx + (D == 0), fh = ny + (D == 1);
   const int E[3] = {nx + (D != 0), ny + (D != 1), nz + (D != 2)};
   const int nact = B.nfaces[D];

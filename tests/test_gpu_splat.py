@@ -112,3 +112,32 @@ def test_splat_without_particles_and_argument_errors():
     partial.mass[0] = buf[0].ctypes.data
     assert L.shkz_b200_splat_host(ctx.handle, ctypes.byref(partial)) == -1
     assert L.shkz_b200_splat_device(ctx.handle, ctypes.byref(args(particles=P.ctypes.data + 2))) == -1
+
+
+def test_oversized_bucket_is_refused_and_grids_untouched():
+    """More than 4096 particles in one edge bucket (never the case in a FLIP
+    simulation, which keeps 8 to 12 per cell) returns SHKZ_B200_ERR_LIMIT and
+    leaves the caller's grids as they were; the next normal call works."""
+    import ctypes as C
+    from shiokaze_b200 import native, scenes
+    sc = scenes.dambreak_sphere(n=12, seed=1)
+    ctx = native.Context(native.default_config())
+    L = native.load()
+    P = np.zeros(5000, scenes.PARTICLE_DTYPE)
+    P["p"] = np.float32(5.3 * sc.dx)
+    P["mass"] = np.float32(0.125)
+    vel = [np.ascontiguousarray(v).copy() for v in sc.velocity_effective()]
+    act = [m.astype(np.uint8) for m in sc.velocity_active]
+    before = [v.copy() for v in vel], [m.copy() for m in act]
+    a = native.splat_args(sc.nx, sc.ny, sc.nz, sc.dx, P.ctypes.data, len(P), P.dtype)
+    for d in range(3):
+        a.velocity[d], a.velocity_active[d] = vel[d].ctypes.data, act[d].ctypes.data
+    assert L.shkz_b200_splat_host(ctx.handle, C.byref(a)) == -8
+    for d in range(3):
+        assert np.array_equal(vel[d].view(np.uint32), before[0][d].view(np.uint32))
+        assert np.array_equal(act[d], before[1][d])
+    small = P[:100]
+    v, a_, mass, mom, sact = native.splat(ctx, sc.nx, sc.ny, sc.nz, sc.dx, small, vel, act)
+    want = oracle.splat(sc.nx, sc.ny, sc.nz, sc.dx, small, vel, act)
+    assert_bitexact((v, a_, mass, mom, sact), dict(zip(("velocity", "velocity_active", "mass", "momentum",
+                                                        "splat_active"), want)))
