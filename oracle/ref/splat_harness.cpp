@@ -14,7 +14,12 @@
 //   prints "hash_ms H splat_ms S combine_ms C": wall time of the particle
 //   hash (sort_particles), the splat and the combined velocity
 //   configuration keys go to the reference (APIC=Yes|No,
-//   SplatBulletParticle=Yes|No, ...)
+//   SplatBulletParticle=Yes|No, ...). With FLIP=<module> the splat is that
+//   FLIP module's, loaded by the reference's module loader (e.g. the B200
+//   module macnbflip3_b200): the particles reach it through the reference's
+//   own serialisation (recursive_serialize of the compiled-in macnbflip3, then
+//   recursive_initialize of the module from that file), and the splat runs
+//   through macflip3_interface::splat.
 //
 // Input file (little endian):
 //   char[8] "SHKZSP01"; int32 nx, ny, nz; double dx, time; int64 count;
@@ -29,6 +34,7 @@
 #include <shiokaze/array/macarray3.h>
 #include <shiokaze/core/configuration.h>
 #include <shiokaze/core/credit.h>
+#include <shiokaze/core/filesystem.h>
 #include <chrono>
 #include <cstdio>
 #include <cstring>
@@ -52,6 +58,12 @@ public:
 		sort_particles();
 	}
 	static Particle blank() { return Particle(); }
+};
+//
+// the FLIP module named by the FLIP key, through the reference's loader
+class module_root : public recursive_configurable {
+public:
+	macflip3_driver m_flip{this,"macnbflip3"};
 };
 //
 class splat_root : public recursive_configurable {
@@ -143,8 +155,22 @@ int main( int argc, const char *argv[] ) {
 	//
 	auto &mm = root.m_mass_momentum;
 	mm.initialize(shape);
+	module_root froot;
+	const bool use_module = dict.count("FLIP") > 0;
+	if( use_module ) {
+		const std::string path = std::string(argv[2])+".flip";
+		{
+			filestream out(path,filestream::WRITE);
+			root.m_flip.recursive_serialize(out);
+		}
+		froot.recursive_load(config);
+		froot.recursive_configure(config);
+		filestream in(path,filestream::READ);
+		froot.m_flip->recursive_initialize(in);
+	}
 	const auto t2 = std::chrono::steady_clock::now();
-	root.m_flip.run_splat(time,mm);
+	if( use_module ) froot.m_flip->splat(time,mm);
+	else root.m_flip.run_splat(time,mm);
 	const auto t3 = std::chrono::steady_clock::now();
 	//
 	// combined grid velocity: every value is computed from the velocity

@@ -124,12 +124,15 @@ def run_reference(scene, variant: str = "float", mode: str = "mic0", tol: Option
 
 def run_reference_splat(nx: int, ny: int, nz: int, dx: float, particles: np.ndarray, velocity: list,
                         velocity_active: list, apic: bool = True, splat_bullet: bool = False,
-                        time: float = 0.0, variant: str = "float") -> dict:
+                        time: float = 0.0, variant: str = "float", module: Optional[str] = None,
+                        extra_libpath=None) -> dict:
     """Run the compiled reference FLIP splat (``shkz_ref_splat``: macnbflip3::splat
     then the combined grid velocity of macflipliquid3) on particle records in
     the reference's layout. Returns face grids (lists over dim) under
     ``mass``, ``momentum``, ``splat_active``, ``velocity``, ``velocity_active``,
-    and the reference's wall times ``hash_ms``, ``splat_ms``, ``combine_ms``."""
+    and the reference's wall times ``hash_ms``, ``splat_ms``, ``combine_ms``.
+    With ``module``, the splat is that FLIP module's (FLIP=<module>, found on
+    ``extra_libpath``), loaded by the reference's module loader."""
     exe = os.path.join(REF_DIR, variant, "shkz_ref_splat")
     P = np.ascontiguousarray(particles)
     n = len(P)
@@ -147,13 +150,19 @@ def run_reference_splat(nx: int, ny: int, nz: int, dx: float, particles: np.ndar
                 f.write(np.ascontiguousarray(v, np.float32).tobytes())
                 f.write(np.ascontiguousarray(a, np.uint8).tobytes())
         env = dict(os.environ)
-        env["LD_LIBRARY_PATH"] = ":".join([os.path.join(REF_DIR, variant), env.get("LD_LIBRARY_PATH", "")])
+        env["LD_LIBRARY_PATH"] = ":".join(list(extra_libpath or []) + [os.path.join(REF_DIR, variant),
+                                                                       env.get("LD_LIBRARY_PATH", "")])
         args = [exe, fin, fout, "APIC=" + ("Yes" if apic else "No"),
                 "SplatBulletParticle=" + ("Yes" if splat_bullet else "No")]
+        if module:
+            args.append("FLIP=" + module)
         proc = subprocess.run(args, cwd=td, env=env, capture_output=True, text=True)
         if proc.returncode != 0:
             raise RuntimeError(f"reference splat failed ({proc.returncode}):\n{proc.stdout[-2000:]}\n{proc.stderr[-2000:]}")
         out = {k: [] for k in ("mass", "momentum", "splat_active", "velocity", "velocity_active")}
+        if not os.path.exists(fout):
+            # the module loader ends the process with status 0 when a module is missing
+            raise RuntimeError(f"reference splat wrote no output:\n{proc.stdout[-2000:]}\n{proc.stderr[-2000:]}")
         m = re.search(r"hash_ms ([0-9.]+) splat_ms ([0-9.]+) combine_ms ([0-9.]+)", proc.stdout)
         if m:
             out["hash_ms"], out["splat_ms"], out["combine_ms"] = (float(x) for x in m.groups())

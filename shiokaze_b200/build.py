@@ -65,7 +65,13 @@ def build(verbose: bool = False, extra=None) -> str:
 
 
 PLUGINS = {"libshiokaze_macpressuresolver3_b200.so": "macpressuresolver3_b200.cpp",
-           "libshiokaze_pcg_b200.so": "pcg_b200.cpp"}
+           "libshiokaze_pcg_b200.so": "pcg_b200.cpp",
+           "libshiokaze_macnbflip3_b200.so": "macnbflip3_b200.cpp"}
+
+# modules that subclass a reference module compile its source from the
+# reference tree (include path of that source file, and the file itself as
+# a dependency)
+PLUGIN_REFERENCE_SOURCES = {"macnbflip3_b200.cpp": "src/flip/macnbflip3.cpp"}
 
 
 def build_plugins(reference_root: str, verbose: bool = False) -> list:
@@ -81,11 +87,17 @@ def build_plugins(reference_root: str, verbose: bool = False) -> list:
     for so, src in PLUGINS.items():
         target = os.path.join(HERE, so)
         source = os.path.join(HERE, "plugin", src)
-        if _stale(target, [source, lib, os.path.join(HERE, "..", "include", "shkz_b200.h")]):
+        deps = [source, lib, os.path.join(HERE, "..", "include", "shkz_b200.h")]
+        extra_inc = []
+        if src in PLUGIN_REFERENCE_SOURCES:
+            ref_src = os.path.join(reference_root, PLUGIN_REFERENCE_SOURCES[src])
+            deps.append(ref_src)
+            extra_inc = ["-I" + os.path.dirname(ref_src)]
+        if _stale(target, deps):
             cmd = ["g++", "-std=c++17", "-O3", "-fPIC", "-shared", "-w",
                    '-DSHKZ_SUFFIX=""', "-DSHKZ_RELEASE=1", f"-DNUM_THREAD={os.cpu_count() or 4}",
                    "-I" + inc, "-I" + os.path.join(reference_root, "local", "include"),
-                   "-I" + os.path.join(HERE, "..", "include"), source, "-o", target,
+                   "-I" + os.path.join(HERE, "..", "include")] + extra_inc + [source, "-o", target,
                    "-L" + HERE, "-lshkz_b200", "-Wl,-rpath,$ORIGIN"]
             if verbose:
                 print(" ".join(cmd), flush=True)

@@ -1,7 +1,9 @@
-"""The Shiokaze module libshiokaze_macpressuresolver3_b200.so loaded by the
-reference's own module loader (Projection=macpressuresolver3_b200) inside the
-compiled reference harness, against Projection=macpressuresolver3 on the same
-grids. This is the drop-in path a Shiokaze user takes."""
+"""The Shiokaze modules loaded by the reference's own module loader inside the
+compiled reference harnesses: libshiokaze_macpressuresolver3_b200.so
+(Projection=macpressuresolver3_b200) against Projection=macpressuresolver3 on
+the same grids, libshiokaze_pcg_b200.so (LinSolver=pcg_b200), and
+libshiokaze_macnbflip3_b200.so (FLIP=macnbflip3_b200) against the reference
+macnbflip3's splat. This is the drop-in path a Shiokaze user takes."""
 import os
 
 import numpy as np
@@ -112,3 +114,26 @@ def test_streamfunc_projection_runs_on_pcg_b200(n, seed, tol):
         m = ref.velocity_active[d] != 0
         assert np.abs(ref.velocity[d][m] - vin[d][m]).max() > 1e-2
         assert rel_inf(got.velocity[d], ref.velocity[d]) <= tol_v, (d, rel_inf(got.velocity[d], ref.velocity[d]))
+
+
+FLIP_PLUGIN = os.path.join(PKG, "libshiokaze_macnbflip3_b200.so")
+
+
+@pytest.mark.skipif(not (os.path.exists(os.path.join(ref_runner.REF_DIR, "float", "shkz_ref_splat"))
+                         and os.path.exists(FLIP_PLUGIN)),
+                    reason="needs the compiled reference splat harness and the FLIP module")
+def test_flip_module_splat_matches_reference(golden_splat):
+    """FLIP=macnbflip3_b200 loaded by the reference's module loader, its
+    particles handed over by the reference's own serialisation, splatting
+    through macflip3_interface::splat: the splat grid and the combined
+    velocity are bit-identical to the reference macnbflip3's."""
+    from conftest import splat_particles
+    from test_oracle_splat import assert_bitexact, reference_outputs
+    name, g = golden_splat
+    nx, ny, nz = (int(v) for v in g["shape"])
+    r = ref_runner.run_reference_splat(nx, ny, nz, float(g["dx"]), splat_particles(g), [g["u0"], g["v0"], g["w0"]],
+                                       [g["u0_active"], g["v0_active"], g["w0_active"]], apic=bool(g["apic"]),
+                                       splat_bullet=bool(g["splat_bullet"]), module="macnbflip3_b200",
+                                       extra_libpath=[PKG])
+    got = [r[k] for k in ("velocity", "velocity_active", "mass", "momentum", "splat_active")]
+    assert_bitexact(got, reference_outputs(g))
