@@ -244,9 +244,9 @@ typedef struct shkz_b200_splat_args {
 /* Host buffers (particle records and grids copied to the device and back). */
 int shkz_b200_splat_host(shkz_b200_ctx *ctx, const shkz_b200_splat_args *args);
 
-/* Device pointers on the context's device (the particle records 4-byte
- * aligned): the grid velocity can go straight on to
- * shkz_b200_project_device. */
+/* Device pointers on the context's device (the particle records and the
+ * float face grids 4-byte aligned, else SHKZ_B200_ERR_ARG): the grid velocity
+ * can go straight on to shkz_b200_project_device. */
 int shkz_b200_splat_device(shkz_b200_ctx *ctx, const shkz_b200_splat_args *args);
 
 /* The CUDA stream the context launches on (as an opaque pointer), so callers

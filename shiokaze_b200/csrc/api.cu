@@ -1154,7 +1154,11 @@ extern "C" int shkz_b200_splat_device(shkz_b200_ctx *ctx, const shkz_b200_splat_
   if (!ctx) return SHKZ_B200_ERR_ARG;
   int rc = validate_splat(a);
   if (rc) return rc;
-  if (a->count && ((uintptr_t)a->particles & 3u)) return SHKZ_B200_ERR_ARG;
+  // the kernels read the records' floats and write the face floats 4 bytes at a time
+  auto aligned4 = [](const void *p) { return ((uintptr_t)p & 3u) == 0; };
+  if (a->count && !aligned4(a->particles)) return SHKZ_B200_ERR_ARG;
+  for (int d = 0; d < 3; ++d)
+    if (!aligned4(a->velocity[d]) || !aligned4(a->mass[d]) || !aligned4(a->momentum[d])) return SHKZ_B200_ERR_ARG;
   cudaSetDevice(ctx->device);
   SplatGrid G{};
   for (int d = 0; d < 3; ++d) {

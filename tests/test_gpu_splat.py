@@ -112,6 +112,9 @@ def test_splat_without_particles_and_argument_errors():
     partial.mass[0] = buf[0].ctypes.data
     assert L.shkz_b200_splat_host(ctx.handle, ctypes.byref(partial)) == -1
     assert L.shkz_b200_splat_device(ctx.handle, ctypes.byref(args(particles=P.ctypes.data + 2))) == -1
+    shifted = args()
+    shifted.velocity[1] = buf[1].ctypes.data + 2
+    assert L.shkz_b200_splat_device(ctx.handle, ctypes.byref(shifted)) == -1
 
 
 def test_oversized_bucket_is_refused_and_grids_untouched():
