@@ -313,11 +313,15 @@ def run_splat(args):
     algo = SPLAT_BYTES_PARTICLE * len(P) + SPLAT_BYTES_FACE * faces
     peak, peak_kind = measured_peaks()
     achieved = algo / (call_ms * 1e-3) / 1e9
+    t0 = (ncu_traffic() or {}).get("splat_call")
+    traffic = t0["dram_bytes_per_launch"] * len(P) / t0["particles"] if t0 else None
     roofline = {"kernel": "shkz_b200_splat_device (bin, scan, bucket sort, face lists, k_splat_gather x3)",
                 "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "peak_kind": peak_kind, "ms": call_ms, "algo_bytes_per_launch": algo, "traffic": None,
-                "note": ("not HBM-bound: the gather (about 3/4 of the call) is bound by FP64 issue and lane "
-                         "divergence, each face summing its particles serially in the reference's order")}
+                "peak_kind": peak_kind, "ms": call_ms, "algo_bytes_per_launch": algo, "traffic": traffic,
+                "note": ("not HBM-bound: the gather (about 3/5 of the call) is bound by FP64 issue and latency, "
+                         "each face summing its particles serially in the reference's order; traffic is 14x the "
+                         "algorithmic bytes because of the hash (bucket counters over the edge grids, packed and "
+                         "bucket-ordered particle copies)")}
     # end to end through the host-buffer entry point, pinned host arrays
     pin = lambda arr: torch.from_numpy(np.ascontiguousarray(arr)).pin_memory()
     h_rec = pin(P.view(np.uint8))
