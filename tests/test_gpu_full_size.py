@@ -74,3 +74,18 @@ def test_full_size_projection_properties(name):
     ref = json.load(open(REF))[name]
     assert res["unknowns"] == ref["unknowns"]
     assert abs(res["iterations"] - ref["iterations"]) <= spread * ref["iterations"], (res["iterations"], ref)
+
+
+def test_full_size_splat_bitexact_against_reference_digest():
+    """The FLIP splat at the splat benchmark's size (256^3 tank, 2.4 M
+    particles) through shkz_b200_splat_host: its outputs hash to the digest
+    of the compiled reference's outputs."""
+    from golden.make_full_size import splat_case, splat_digest
+    from shiokaze_b200 import native
+    ref = json.load(open(REF))["splat_sloshing_tank_256"]
+    sc, P = splat_case()
+    ctx = native.Context(native.default_config())
+    out = native.splat(ctx, sc.nx, sc.ny, sc.nz, sc.dx, P, sc.velocity_effective(),
+                       [m.astype(np.uint8) for m in sc.velocity_active])
+    assert sum(int(s.sum()) for s in out[4]) == ref["splatted_faces"]
+    assert splat_digest(*out) == ref["splat_digest"]

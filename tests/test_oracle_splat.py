@@ -87,3 +87,21 @@ def test_narrow_band_particles():
     full = scenes.flip_particles(sc, per_cell=2, seed=0, edge_cases=False)
     band = scenes.flip_particles(sc, per_cell=2, seed=0, edge_cases=False, band=3.0)
     assert 0 < len(band) < len(full)
+
+
+def test_oracle_splat_full_size_digest():
+    """The splat benchmark's workload (256^3 tank, 2.4 M particles in the
+    3-cell band): the CPU restatement's outputs hash to the digest the
+    compiled reference's outputs were recorded with (tests/golden/
+    make_full_size.py)."""
+    import json
+    from conftest import GOLDEN
+    from golden.make_full_size import splat_case, splat_digest
+    import os
+    ref = json.load(open(os.path.join(GOLDEN, "full_size_reference.json")))["splat_sloshing_tank_256"]
+    sc, P = splat_case()
+    assert len(P) == ref["particles"]
+    v, a, mass, mom, sact = oracle.splat(sc.nx, sc.ny, sc.nz, sc.dx, P, sc.velocity_effective(),
+                                         [m.astype(np.uint8) for m in sc.velocity_active])
+    assert sum(int(s.sum()) for s in sact) == ref["splatted_faces"]
+    assert splat_digest(v, a, mass, mom, sact) == ref["splat_digest"]
