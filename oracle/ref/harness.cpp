@@ -21,6 +21,8 @@
 //                              w layers with macarray_extrapolator3::extrapolate
 //                              (include/shiokaze/array/macarray_extrapolator3.h)
 //   HarnessConstrain=1         then macutility3::constrain_velocity(solid, velocity)
+//   HarnessProject=0           no projection (the extension then runs on the
+//                              input velocity; the pressure is written empty)
 //   Projection=<module>        any projection module (default macpressuresolver3;
 //                              macstreamfuncsolver3 has no pressure grid, which is
 //                              then written as empty)
@@ -224,8 +226,9 @@ int main( int argc, const char *argv[] ) {
 	for( int dim=0; dim<3; ++dim ) dump_cells(velocity[dim],shape.face(dim));
 	//
 	const int repeat = dict.count("HarnessRepeat") ? std::atoi(dict["HarnessRepeat"].c_str()) : 1;
-	double best_ms = 1e300;
-	for( int rep=0; rep<std::max(1,repeat); ++rep ) {
+	const bool project = ! dict.count("HarnessProject") || std::atoi(dict["HarnessProject"].c_str());
+	double best_ms = project ? 1e300 : 0.0;
+	for( int rep=0; project && rep<std::max(1,repeat); ++rep ) {
 		if( rep ) set_velocity();
 		if( has_volume ) root.m_macproject->set_target_volume(vol_cur,vol_tgt);
 		auto t0 = std::chrono::steady_clock::now();
@@ -244,7 +247,7 @@ int main( int argc, const char *argv[] ) {
 	//
 	// a projection without a pressure grid (macstreamfuncsolver3::get_pressure
 	// returns nullptr) is written as an empty, inactive grid
-	const array3<Real> *pressure_ptr = root.m_macproject->get_pressure();
+	const array3<Real> *pressure_ptr = project ? root.m_macproject->get_pressure() : nullptr;
 	if( ! pressure_ptr ) {
 		root.m_no_pressure.initialize(shape);
 		pressure_ptr = &root.m_no_pressure;

@@ -5,7 +5,10 @@ run the reference themselves in the time a test has:
 * iteration counts of MIC(0)-PCG to 1e-6 (sloshing tank 256^3, splash 384^3);
 * the FLIP splat of the splat benchmark's workload (sloshing tank 256^3,
   2.4 M particles in the 3-cell narrow band): a SHA-256 of its outputs
-  (``splat_digest``), so the device result can be compared bit for bit.
+  (``splat_digest``), so the device result can be compared bit for bit;
+* the velocity extension (3 passes + constrain_velocity) of the 256^3 tank's
+  input velocity, without a projection: a SHA-256 of the extended velocity
+  and masks (``extend_digest``).
 
 Runs the reference's own ``macpressuresolver3::project`` (built by
 ``oracle/ref/Makefile`` into ``oracle/_ref``); needs the reference sources,
@@ -40,6 +43,23 @@ def splat_digest(velocity, velocity_active, mass, momentum, splat_active) -> str
     return h.hexdigest()
 
 
+def extend_digest(velocity, velocity_active) -> str:
+    """SHA-256 over the extended field, axis by axis: values (float32, only
+    where active) and masks (uint8)."""
+    import hashlib
+    import numpy as np
+    h = hashlib.sha256()
+    for d in range(3):
+        m = np.ascontiguousarray(velocity_active[d], np.uint8)
+        v = np.where(m != 0, np.asarray(velocity[d], np.float32), np.float32(0))
+        h.update(np.ascontiguousarray(v, np.float32).tobytes())
+        h.update(m.tobytes())
+    return h.hexdigest()
+
+
+EXTEND_WIDTH = 3
+
+
 def splat_case():
     sc = scenes.sloshing_tank(n=256, seed=0, tol=1e-6)
     return sc, scenes.flip_particles(sc, per_cell=8, seed=0, band=3.0)
@@ -66,6 +86,15 @@ def main():
             "splat_digest": splat_digest(r["velocity"], r["velocity_active"], r["mass"], r["momentum"],
                                          r["splat_active"])}
         print("splat_sloshing_tank_256", out["splat_sloshing_tank_256"], flush=True)
+    if not only or "extend_sloshing_tank_256" in only:
+        sc = scenes.sloshing_tank(n=256, seed=0, tol=1e-6)
+        r = ref_runner.run_reference(sc, mode="mic0", dump_system=False,
+                                     extra={"HarnessProject": 0, "HarnessExtend": EXTEND_WIDTH, "HarnessConstrain": 1})
+        out["extend_sloshing_tank_256"] = {
+            "width": EXTEND_WIDTH, "constrain": 1,
+            "active_faces": int(sum(int(np.asarray(a).sum()) for a in r.velocity_active)),
+            "extend_digest": extend_digest([np.asarray(v, np.float32) for v in r.velocity], r.velocity_active)}
+        print("extend_sloshing_tank_256", out["extend_sloshing_tank_256"], flush=True)
     for name, build in CASES.items():
         if only and name not in only:
             continue

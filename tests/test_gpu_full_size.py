@@ -89,3 +89,18 @@ def test_full_size_splat_bitexact_against_reference_digest():
                        [m.astype(np.uint8) for m in sc.velocity_active])
     assert sum(int(s.sum()) for s in out[4]) == ref["splatted_faces"]
     assert splat_digest(*out) == ref["splat_digest"]
+
+
+def test_full_size_extension_bitexact_against_reference_digest():
+    """The velocity extension at 256^3 (3 passes + constraint on the tank's
+    input velocity) through shkz_b200_extend_velocity_host: the result hashes
+    to the digest of the compiled reference's."""
+    from golden.make_full_size import EXTEND_WIDTH, extend_digest
+    from shiokaze_b200 import native, scenes
+    ref = json.load(open(REF))["extend_sloshing_tank_256"]
+    sc = scenes.sloshing_tank(n=256, seed=0, tol=1e-6)
+    ctx = native.Context(native.default_config())
+    v, a = native.extend_velocity(ctx, sc.velocity_effective(), [m.astype(np.uint8) for m in sc.velocity_active],
+                                  sc.solid_effective(), sc.solid_active.astype(np.uint8), sc.dx, EXTEND_WIDTH, True)
+    assert sum(int(m.sum()) for m in a) == ref["active_faces"]
+    assert extend_digest(v, a) == ref["extend_digest"]

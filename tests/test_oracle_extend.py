@@ -47,3 +47,20 @@ def test_oracle_extension_matches_compiled_reference(width, constrain):
     v, a = ext.extend(r0.velocity, r0.velocity_active, r0.solid.astype(np.float32), r0.solid_active, sc.dx,
                       width, bool(constrain))
     assert_same_extension(v, a, r1.velocity, r1.velocity_active)
+
+
+def test_oracle_extension_full_size_digest():
+    """The 256^3 tank's input velocity extended 3 passes and constrained (no
+    projection before it): the CPU restatement hashes to the digest of the
+    compiled reference's result (tests/golden/make_full_size.py)."""
+    import json
+    import os
+    from conftest import GOLDEN
+    from golden.make_full_size import EXTEND_WIDTH, extend_digest
+    from shiokaze_b200 import scenes
+    ref = json.load(open(os.path.join(GOLDEN, "full_size_reference.json")))["extend_sloshing_tank_256"]
+    sc = scenes.sloshing_tank(n=256, seed=0, tol=1e-6)
+    v, a = ext.extend(sc.velocity_effective(), [m.astype(np.uint8) for m in sc.velocity_active],
+                      sc.solid_effective(), sc.solid_active, sc.dx, EXTEND_WIDTH, True)
+    assert sum(int(np.asarray(m).sum()) for m in a) == ref["active_faces"]
+    assert extend_digest(v, a) == ref["extend_digest"]
