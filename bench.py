@@ -526,6 +526,39 @@ def run_liquid_step(args):
     return 0
 
 
+def time_neighbours(ctx, L, sc, stream, dev, vel, vact, solid, sact, reps: int = 20):
+    """Device time of the FLIP splat (3-cell band, 8 particles per cell) and
+    of the velocity extension (3 passes + constraint) on the headline grid,
+    CUDA events on the context stream, after one warm-up call each."""
+    import torch
+    from shiokaze_b200 import native, scenes
+    P = scenes.flip_particles(sc, per_cell=8, seed=0, band=3.0)
+    rec = torch.from_numpy(np.ascontiguousarray(P.view(np.uint8))).to(dev)
+    sp = native.splat_args(sc.nx, sc.ny, sc.nz, sc.dx, rec.data_ptr(), len(P), P.dtype, apic=True)
+    ea = native.ExtendArgs()
+    ea.nx, ea.ny, ea.nz, ea.dx, ea.width, ea.constrain = sc.nx, sc.ny, sc.nz, sc.dx, 3, 1
+    ea.solid, ea.solid_active = solid.data_ptr(), sact.data_ptr()
+    for d in range(3):
+        sp.velocity[d], sp.velocity_active[d] = vel[d].data_ptr(), vact[d].data_ptr()
+        ea.velocity[d], ea.velocity_active[d] = vel[d].data_ptr(), vact[d].data_ptr()
+    out = {"particles": len(P)}
+    for name, fn, a_ in (("splat", L.shkz_b200_splat_device, sp), ("extend", L.shkz_b200_extend_velocity_device, ea)):
+        ctx.check(fn(ctx.handle, ctypes.byref(a_)), name)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            ctx.check(fn(ctx.handle, ctypes.byref(a_)), name)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        out[f"{name}_ms"] = e0.elapsed_time(e1) / reps
+    out["what"] = ("splat: shkz_b200_splat_device (macnbflip3::splat + combined velocity); extend: "
+                   "shkz_b200_extend_velocity_device (3 passes + constrain_velocity); both repeated on the "
+                   "projected velocity, untimed in the headline value")
+    del rec
+    return out
+
+
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -587,6 +620,8 @@ def main():
                     help="sloshing_tank 256^3 (headline), splash 384^3, dambreak_rain 512^3, dambreak_sphere 64^3")
     ap.add_argument("--learned-steps", type=int, default=2,
                     help="timed projections of the learned-preconditioner arm (0: skip)")
+    ap.add_argument("--no-neighbours", dest="neighbours", action="store_false",
+                    help="skip the splat and extension timings added to the headline line")
     ap.add_argument("--workload", default="projection", choices=["projection", "flip_splat", "liquid_step"],
                     help="projection (headline), the FLIP splat before it, or splat + projection + extension")
     args = ap.parse_args()
@@ -860,6 +895,15 @@ def main():
         cfg.preconditioner = native.PRECOND_MIC0
         ctx.set_config(cfg)
 
+    # the projection's timestep neighbours on the same grid (untimed in the
+    # headline): the FLIP splat before it and the velocity extension after it
+    neighbours = None
+    if rank == 0 and args.scene == "sloshing_tank" and args.neighbours:
+        try:
+            neighbours = time_neighbours(ctx, L, sc, stream, dev, vel, vact, solid, sact)
+        except Exception as exc:  # reported in the line, not hidden
+            neighbours = {"error": str(exc)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -884,7 +928,7 @@ def main():
             "phase_ms": {"assemble": last["ms_assemble"], "solve": last["ms_solve"], "update": last["ms_update"]},
             "ms_per_iteration": last["ms_solve"] / max(1, last["iterations"]),
             "e2e": e2e, "roofline": roofline, "roofline_kernels": rooflines, "roofline_iteration": iteration_roofline,
-            "error_vs_fp64": fp64, "learned": learned,
+            "error_vs_fp64": fp64, "learned": learned, "neighbours": neighbours,
             "kernels": kern, "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
         }
         print(json.dumps(line), flush=True)
