@@ -217,7 +217,9 @@ int shkz_b200_extend_velocity_device(shkz_b200_ctx *ctx, const shkz_b200_extend_
  * splat_bullet != 0 (SplatBulletParticle). Face grids use the layouts of
  * shkz_b200_project_args. mass, momentum and splat_active are optional outputs
  * (all three or none): the splat grid itself, zero and inactive where the
- * splatted mass is zero. nx, ny, nz >= 1; the three axes' edge grids together
+ * splatted mass is zero. velocity and velocity_active may be NULL (all of
+ * them) when the splat grid is asked for: the splat alone, as
+ * macflip3_interface::splat returns it, without the combined velocity. nx, ny, nz >= 1; the three axes' edge grids together
  * and 3 * count stay below 2^31. An edge bucket (the particles whose
  * positions round to one edge cell; about 8 to 12 in a FLIP simulation) of
  * more than 4096 particles returns SHKZ_B200_ERR_LIMIT with the grids left
@@ -234,8 +236,8 @@ typedef struct shkz_b200_splat_args {
   int offset_apic;                /* float[3][3], row d = c[d]; -1: APIC off */
   int offset_bullet;              /* uint8 (nonzero = bullet); -1: none */
   int splat_bullet;
-  float *velocity[3];             /* faces, in/out */
-  uint8_t *velocity_active[3];    /* faces, in/out */
+  float *velocity[3];             /* faces, in/out, optional (see above) */
+  uint8_t *velocity_active[3];    /* faces, in/out, optional */
   float *mass[3];                 /* faces, out, optional */
   float *momentum[3];             /* faces, out, optional */
   uint8_t *splat_active[3];       /* faces, out, optional */

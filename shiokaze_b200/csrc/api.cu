@@ -1057,13 +1057,17 @@ static int validate_splat(const shkz_b200_splat_args *a) {
   long long base[3];
   const long long buckets = splat_buckets(a->nx, a->ny, a->nz, base);
   if (buckets + 1 >= ((long long)1 << 31) || 3 * a->count >= ((long long)1 << 31)) return SHKZ_B200_ERR_LIMIT;
+  // the velocity (in/out) and the splat grid (out) are each all three axes or
+  // none, and at least one of them is given
+  const bool vel0 = a->velocity[0] != nullptr;
   for (int d = 0; d < 3; ++d)
-    if (!a->velocity[d] || !a->velocity_active[d]) return SHKZ_B200_ERR_ARG;
+    if ((a->velocity[d] != nullptr) != vel0 || (a->velocity_active[d] != nullptr) != vel0) return SHKZ_B200_ERR_ARG;
   const bool out0 = a->mass[0] != nullptr;
   for (int d = 0; d < 3; ++d)
     if ((a->mass[d] != nullptr) != out0 || (a->momentum[d] != nullptr) != out0 ||
         (a->splat_active[d] != nullptr) != out0)
       return SHKZ_B200_ERR_ARG;
+  if (!vel0 && !out0) return SHKZ_B200_ERR_ARG;
   if (a->count == 0) return 0;
   if (!a->particles || a->stride < 4 || (a->stride & 3)) return SHKZ_B200_ERR_ARG;
   auto field = [&](int off, int bytes) { return off >= 0 && (off & 3) == 0 && off + bytes <= a->stride; };
@@ -1190,12 +1194,15 @@ extern "C" int shkz_b200_splat_host(shkz_b200_ctx *ctx, const shkz_b200_splat_ar
   const bool outs = a->mass[0] != nullptr;
   SplatGrid D{};
   size_t nf[3];
+  const bool vel = a->velocity[0] != nullptr;
   for (int d = 0; d < 3; ++d) {
     nf[d] = (size_t)(a->nx + (d == 0)) * (a->ny + (d == 1)) * (a->nz + (d == 2));
-    SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->h_vel[d], a->velocity[d], nf[d] * 4, cudaMemcpyHostToDevice, s));
-    SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->h_vact[d], a->velocity_active[d], nf[d], cudaMemcpyHostToDevice, s));
-    D.velocity[d] = ctx->h_vel[d];
-    D.velocity_active[d] = ctx->h_vact[d];
+    if (vel) {
+      SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->h_vel[d], a->velocity[d], nf[d] * 4, cudaMemcpyHostToDevice, s));
+      SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->h_vact[d], a->velocity_active[d], nf[d], cudaMemcpyHostToDevice, s));
+      D.velocity[d] = ctx->h_vel[d];
+      D.velocity_active[d] = ctx->h_vact[d];
+    }
     if (outs) {
       if (nf[d] > ctx->cap_sp_out[d]) {
         GROW(sp_mass[d], nf[d]);
@@ -1211,8 +1218,10 @@ extern "C" int shkz_b200_splat_host(shkz_b200_ctx *ctx, const shkz_b200_splat_ar
   rc = splat_device(ctx, a, ctx->sp_raw, D);
   if (rc) return rc;
   for (int d = 0; d < 3; ++d) {
-    SHKZ_CUDA_TRY(cudaMemcpyAsync(a->velocity[d], ctx->h_vel[d], nf[d] * 4, cudaMemcpyDeviceToHost, s));
-    SHKZ_CUDA_TRY(cudaMemcpyAsync(a->velocity_active[d], ctx->h_vact[d], nf[d], cudaMemcpyDeviceToHost, s));
+    if (vel) {
+      SHKZ_CUDA_TRY(cudaMemcpyAsync(a->velocity[d], ctx->h_vel[d], nf[d] * 4, cudaMemcpyDeviceToHost, s));
+      SHKZ_CUDA_TRY(cudaMemcpyAsync(a->velocity_active[d], ctx->h_vact[d], nf[d], cudaMemcpyDeviceToHost, s));
+    }
     if (outs) {
       SHKZ_CUDA_TRY(cudaMemcpyAsync(a->mass[d], ctx->sp_mass[d], nf[d] * 4, cudaMemcpyDeviceToHost, s));
       SHKZ_CUDA_TRY(cudaMemcpyAsync(a->momentum[d], ctx->sp_mom[d], nf[d] * 4, cudaMemcpyDeviceToHost, s));

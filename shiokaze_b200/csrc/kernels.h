@@ -91,7 +91,7 @@ struct SplatBuffers {
   int apic;
 };
 struct SplatGrid {
-  float *velocity[3];
+  float *velocity[3];            // optional (velocity[0] == nullptr: no combined velocity)
   uint8_t *velocity_active[3];
   float *mass[3], *momentum[3];  // optional (mass[0] == nullptr: none)
   uint8_t *splat_active[3];

@@ -497,7 +497,7 @@ __global__ void __launch_bounds__(kGatherThreads) k_splat_gather(int nx, int ny,
       G.momentum[D][f] = on ? mom : 0.0f;
       G.splat_active[D][f] = on ? 1 : 0;
     }
-    if (on) {
+    if (on && G.velocity[D]) {
       // combined grid velocity (macflipliquid3.cpp:141-150)
       float *u = G.velocity[D];
       uint8_t *ua = G.velocity_active[D];

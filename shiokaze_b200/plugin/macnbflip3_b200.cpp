@@ -70,10 +70,10 @@ protected:
 			if( rc ) { fail("shkz_b200_create",rc); return; }
 		}
 		const shape3 s = m_shape;
-		// the combined velocity the entry point also forms is not used here:
-		// its grid is a zero, inactive scratch field
-		std::vector<float> u[3], mass[3], momentum[3];
-		std::vector<uint8_t> u_active[3], splat_active[3];
+		// the splat grid only (no velocity: the entry point then forms no
+		// combined velocity and copies no velocity grid)
+		std::vector<float> mass[3], momentum[3];
+		std::vector<uint8_t> splat_active[3];
 		shkz_b200_splat_args a;
 		std::memset(&a,0,sizeof(a));
 		a.nx = s.w; a.ny = s.h; a.nz = s.d; a.dx = m_dx;
@@ -88,9 +88,7 @@ protected:
 		a.splat_bullet = m_param.splat_bullet_particle ? 1 : 0;
 		for( int dim : DIMS3 ) {
 			const size_t nf = s.face(dim).count();
-			u[dim].assign(nf,0.0f); u_active[dim].assign(nf,0);
 			mass[dim].assign(nf,0.0f); momentum[dim].assign(nf,0.0f); splat_active[dim].assign(nf,0);
-			a.velocity[dim] = u[dim].data(); a.velocity_active[dim] = u_active[dim].data();
 			a.mass[dim] = mass[dim].data(); a.momentum[dim] = momentum[dim].data();
 			a.splat_active[dim] = splat_active[dim].data();
 		}

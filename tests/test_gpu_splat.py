@@ -144,3 +144,31 @@ def test_oversized_bucket_is_refused_and_grids_untouched():
     want = oracle.splat(sc.nx, sc.ny, sc.nz, sc.dx, small, vel, act)
     assert_bitexact((v, a_, mass, mom, sact), dict(zip(("velocity", "velocity_active", "mass", "momentum",
                                                         "splat_active"), want)))
+
+
+def test_splat_grid_alone_without_velocity(golden_splat):
+    """Velocity pointers NULL: the entry point returns the splat grid alone
+    (what macflip3_interface::splat hands back), bit-identical to the
+    reference's; with neither the velocity nor the splat grid the call is
+    refused."""
+    from shiokaze_b200 import native
+    name, g = golden_splat
+    nx, ny, nz = (int(v) for v in g["shape"])
+    P = splat_particles(g)
+    want = reference_outputs(g)
+    ctx = native.Context(native.default_config())
+    L = native.load()
+    mass = [np.zeros_like(np.asarray(x, np.float32)) for x in want["mass"]]
+    mom = [np.zeros_like(m) for m in mass]
+    sact = [np.zeros(m.shape, np.uint8) for m in mass]
+    a = native.splat_args(nx, ny, nz, float(g["dx"]), P.ctypes.data, len(P), P.dtype, apic=bool(g["apic"]),
+                          splat_bullet=bool(g["splat_bullet"]))
+    for d in range(3):
+        a.mass[d], a.momentum[d], a.splat_active[d] = mass[d].ctypes.data, mom[d].ctypes.data, sact[d].ctypes.data
+    ctx.check(L.shkz_b200_splat_host(ctx.handle, ctypes.byref(a)), "splat_host")
+    for d in range(3):
+        assert np.array_equal(sact[d], want["splat_active"][d])
+        assert np.array_equal(mass[d].view(np.uint32), np.asarray(want["mass"][d], np.float32).view(np.uint32))
+        assert np.array_equal(mom[d].view(np.uint32), np.asarray(want["momentum"][d], np.float32).view(np.uint32))
+    b = native.splat_args(nx, ny, nz, float(g["dx"]), P.ctypes.data, len(P), P.dtype)
+    assert L.shkz_b200_splat_host(ctx.handle, ctypes.byref(b)) == -1
