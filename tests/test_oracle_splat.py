@@ -105,3 +105,24 @@ def test_oracle_splat_full_size_digest():
                                          [m.astype(np.uint8) for m in sc.velocity_active])
     assert sum(int(s.sum()) for s in sact) == ref["splatted_faces"]
     assert splat_digest(v, a, mass, mom, sact) == ref["splat_digest"]
+
+
+def test_harness_module_path_reproduces_compiled_in_splat():
+    """The harness's FLIP=<module> path (particles handed to a module loaded
+    by the reference's loader through the reference's own serialisation, then
+    macflip3_interface::splat), run with the reference's own macnbflip3
+    module, gives exactly the compiled-in splat: the path the GPU module is
+    tested through adds nothing of its own."""
+    import os
+    import pytest
+    from oracle import ref_runner
+    if not os.path.exists(os.path.join(ref_runner.REF_DIR, "float", "libshiokaze_macnbflip3.so")):
+        pytest.skip("reference macnbflip3 module not built (needs the reference sources)")
+    sc = scenes.splash(n=20, seed=1, spheres=6)
+    P = scenes.flip_particles(sc, per_cell=3, seed=4, bullet_fraction=0.1)
+    args = (sc.nx, sc.ny, sc.nz, sc.dx, P, sc.velocity_effective(), [m.astype(np.uint8) for m in sc.velocity_active])
+    a = ref_runner.run_reference_splat(*args)
+    b = ref_runner.run_reference_splat(*args, module="macnbflip3")
+    for key in KEYS:
+        for d in range(3):
+            assert np.array_equal(np.asarray(a[key][d]).view(np.uint8), np.asarray(b[key][d]).view(np.uint8)), key
