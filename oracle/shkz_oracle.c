@@ -22,6 +22,11 @@
  *                       discarded at pcg_solver.h:379-384) or the MIC(0)
  *                       factor and sweeps (pcg_solver.h:88-223) applied
  *   - velocity update   macpressuresolver3.cpp:262-284
+ *   - FLIP splat        macnbflip3::splat over the pointgridhash3 edge hash
+ *                       (src/flip/macnbflip3.cpp:103-148,
+ *                       src/pointgridhash/pointgridhash3.cpp:90-100, 218-231)
+ *                       and macflipliquid3's combined velocity
+ *                       (src/liquid/macflipliquid3.cpp:135-151); see shkzo_splat
  *
  * Grids are dense, x fastest: cell (i,j,k) at i + nx*(j + ny*k); nodal grids
  * are (nx+1)*(ny+1)*(nz+1); face grid d has nx+(d==0), ny+(d==1), nz+(d==2).
