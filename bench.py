@@ -27,6 +27,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -118,10 +119,13 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
+    # where the samples go: --clock-log DIR, else the system temp directory
+    LOG_DIR = None
+
     def __init__(self, device: int):
         self.device = device
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
+        self.path = os.path.join(self.LOG_DIR or tempfile.gettempdir(), f"clocks_bench_{os.getpid()}_{device}.csv")
 
     def __enter__(self):
         try:
@@ -622,9 +626,14 @@ def main():
                     help="timed projections of the learned-preconditioner arm (0: skip)")
     ap.add_argument("--no-neighbours", dest="neighbours", action="store_false",
                     help="skip the splat and extension timings added to the headline line")
+    ap.add_argument("--clock-log", default=None,
+                    help="directory for the nvidia-smi clock samples of the timed region (default: temp dir)")
     ap.add_argument("--workload", default="projection", choices=["projection", "flip_splat", "liquid_step"],
                     help="projection (headline), the FLIP splat before it, or splat + projection + extension")
     args = ap.parse_args()
+    if args.clock_log:
+        os.makedirs(args.clock_log, exist_ok=True)
+        ClockSampler.LOG_DIR = args.clock_log
     if args.workload == "liquid_step":
         args.warmup = max(args.warmup, 3)
         return run_liquid_step(args)

@@ -297,7 +297,7 @@ int shkz_b200_apply_matrix(shkz_b200_ctx *ctx, const float *x_cells, float *y_ce
  * roofline figures. */
 int shkz_b200_time_kernel(shkz_b200_ctx *ctx, int which, int reps, double *ms_per_launch, long long *cells_out);
 
-/* ---- learned preconditioner (conv encoder-decoder, see DESIGN) ----
+/* ---- learned preconditioner (3-level conv encoder-decoder used in a flexible PCG) ----
  * No counterpart in the reference: the network is the second preconditioner
  * of the projection (config preconditioner = SHKZ_B200_PRECOND_LEARNED);
  * the entry points below create, train, inspect and persist it. Training and
@@ -330,7 +330,10 @@ int shkz_b200_learned_save(shkz_b200_ctx *ctx, const char *path);
  * resolution (nz/2,ny/2,nx/2,c1) nearest-upsampled and concatenated (may be
  * NULL when c1 = 0), w[27][cout][c0+c1], bias[cout] (may be NULL), planes = 4
  * or 8 output z planes per CTA; out (nz,ny,nx,cout). c0, c1 multiples of 16,
- * cout <= 128, even grid sizes. No reference counterpart. */
+ * cout <= 128, even grid sizes. The accumulators of one CTA take planes x
+ * (cout rounded up to a power of two, at least 32) tensor-memory columns, at
+ * most 512: planes = 8 allows cout <= 64; a larger product returns
+ * SHKZ_B200_ERR_LIMIT before any device work. No reference counterpart. */
 int shkz_b200_conv3d(int nx, int ny, int nz, int c0, int c1, int cout, int planes, const float *in0,
                      const float *in1, const float *w, const float *bias, int relu, float *out);
 
@@ -342,11 +345,15 @@ int shkz_b200_conv3d(int nx, int ny, int nz, int c0, int c1, int cout, int plane
  * (nz/2,ny/2,nx/2,c1) BF16 bit patterns channels-last, w[27][cout][c0+c1]
  * FP32, bias[cout] FP32 (may be NULL), out (nz,ny,nx,cout) BF16 bit patterns
  * -- and `stream` is a cudaStream_t (NULL = the default stream); the call
- * returns after the stream has drained. Its scratch (packed weights, block
- * flags, an error word) is a fixed 1.1 MiB array in the library that each GPU
- * holds until exit. Limits: cout in {16, 32, 64, 128}, c0 + c1 <= 128 (both
- * multiples of 16), at most 2^18 output blocks of 8x16x8 voxels (a 512^3 grid);
- * larger sizes return SHKZ_B200_ERR_LIMIT. The first call on a device (with
+ * waits for the stream to drain and reads the kernel's error word back before
+ * it returns. in0, in1 and out must start on 16-byte boundaries and w, bias on
+ * 4-byte boundaries (SHKZ_B200_ERR_ARG otherwise). Its scratch (packed
+ * weights, block flags, an error word) is a fixed 1.1 MiB array in the library
+ * that each GPU holds until exit. Limits: cout in {16, 32, 64, 128}, c0 + c1 <=
+ * 128 (both multiples of 16), planes x max(cout, 32) <= 512 tensor-memory
+ * columns (planes = 8 only with cout <= 64), at most 2^18 output blocks of
+ * 8x16x8 voxels (a 512^3 grid); larger sizes return SHKZ_B200_ERR_LIMIT. All
+ * checks come before any device work. The first call on a device (with
  * that device current) looks up the array's device address; make it before
  * any stream capture. Calls share the array, so calls that overlap on the GPU
  * race: serialise them. No counterpart in the reference. */

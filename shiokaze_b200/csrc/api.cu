@@ -1969,5 +1969,11 @@ extern "C" int shkz_b200_conv3d(int nx, int ny, int nz, int c0, int c1, int cout
   if (nx <= 0 || ny <= 0 || nz <= 0 || c0 <= 0 || c0 % 16 || c1 < 0 || c1 % 16 || cout <= 0 || cout > 128 ||
       (planes != 4 && planes != 8) || !in0 || !w || !out || (c1 && !in1) || (nx | ny | nz) & 1)
     return SHKZ_B200_ERR_ARG;
+  // the kernel runs with cout padded to a power of two (at least 16); one
+  // CTA's accumulators take planes x that (each plane on a 32-column
+  // boundary) of the SM's 512 tensor-memory columns
+  int n_pad = 16;
+  while (n_pad < cout) n_pad <<= 1;
+  if (planes * ((n_pad + 31) & ~31) > 512) return SHKZ_B200_ERR_LIMIT;
   return conv3d_run(nx, ny, nz, c0, c1, cout, planes, in0, in1, w, bias, relu, out);
 }

@@ -13,8 +13,9 @@
 // Host code must not hand the array's name to a kernel: on the host it is a
 // stand-in symbol, not a device address. The first call on each device
 // (made with that device current) looks its device address up once with
-// cudaGetSymbolAddress; make that first call before any stream capture. All
-// calls share the array and it keeps the last call's contents: each call
+// cudaGetSymbolAddress; make that first call before any stream capture. Each
+// call waits for its stream to drain and reads the error word back before it
+// returns. All calls share the array and it keeps the last call's contents: each call
 // rewrites the packed weights and the activity bytes it uses and clears the
 // error word. Calls that overlap on the GPU (other streams, other host
 // threads) race on the array; serialise them.
@@ -63,8 +64,17 @@ extern "C" int shkz_b200_conv3d_noalloc(int nx, int ny, int nz, int c0, int c1, 
   if (nx <= 0 || ny <= 0 || nz <= 0 || c0 <= 0 || c0 % 16 || c1 < 0 || c1 % 16 || !in0 || !w || !out ||
       (c1 && !in1) || (c1 && ((nx | ny | nz) & 1)) || (planes != 4 && planes != 8))
     return SHKZ_B200_ERR_ARG;
+  // the kernel's vector loads and stores and its tensor map need 16-byte
+  // aligned activations; the weight packing reads FP32 words
+  const auto misaligned = [](const void *p, uintptr_t a) { return (reinterpret_cast<uintptr_t>(p) & (a - 1)) != 0; };
+  if (misaligned(in0, 16) || (c1 && misaligned(in1, 16)) || misaligned(out, 16) || misaligned(w, 4) ||
+      (bias && misaligned(bias, 4)))
+    return SHKZ_B200_ERR_ARG;
   if (cout != 16 && cout != 32 && cout != 64 && cout != 128) return SHKZ_B200_ERR_LIMIT;
   if (c0 + c1 > kMaxCin) return SHKZ_B200_ERR_LIMIT;
+  // one CTA's accumulators: planes x cout FP32 columns of tensor memory (each
+  // plane on a 32-column boundary), at most the 512 columns of an SM
+  if (planes * ((cout + 31) & ~31) > 512) return SHKZ_B200_ERR_LIMIT;
   const size_t nb = (size_t)((nx + 7) / 8) * ((ny + 15) / 16) * ((nz + 7) / 8);
   if (nb > kMaxBlocks) return SHKZ_B200_ERR_LIMIT;
   int dev = 0;

@@ -70,3 +70,30 @@ def test_ctypes_structs_match_the_header(tmp_path):
         assert got[(cname, "size")] == ctypes.sizeof(py), cname
         for field, _ in py._fields_:
             assert got[(cname, field)] == getattr(py, field).offset, (cname, field)
+
+
+def test_conv_entry_points_reject_before_device_work():
+    """The convolution entry points refuse sizes and pointers they cannot take
+    before they touch the device (these calls run without a GPU): a tensor-
+    memory request above the SM's 512 columns (planes 8 with cout 128), and,
+    for the no-allocation variant, activations or outputs off a 16-byte
+    boundary."""
+    import numpy as np
+    from shiokaze_b200 import native
+    L = native.load()
+    buf = np.zeros(64, np.float32)
+    p = buf.ctypes.data
+    assert p % 16 == 0
+    ERR_ARG, ERR_LIMIT = -1, -8
+    # accumulators of 8 planes x 128 columns = 1024 > 512
+    assert L.shkz_b200_conv3d(16, 32, 16, 16, 0, 128, 8, p, None, p, None, 1, p) == ERR_LIMIT
+    assert L.shkz_b200_conv3d(16, 32, 16, 16, 0, 96, 8, p, None, p, None, 1, p) == ERR_LIMIT
+    assert L.shkz_b200_conv3d_noalloc(16, 32, 16, 16, 0, 128, 8, p, None, p, None, 1, p, None) == ERR_LIMIT
+    # misaligned in0, in1, out (16 bytes) and w (4 bytes)
+    assert L.shkz_b200_conv3d_noalloc(16, 32, 16, 16, 0, 16, 8, p + 8, None, p, None, 1, p, None) == ERR_ARG
+    assert L.shkz_b200_conv3d_noalloc(16, 32, 16, 16, 16, 16, 8, p, p + 4, p, None, 1, p, None) == ERR_ARG
+    assert L.shkz_b200_conv3d_noalloc(16, 32, 16, 16, 0, 16, 8, p, None, p, None, 1, p + 2, None) == ERR_ARG
+    assert L.shkz_b200_conv3d_noalloc(16, 32, 16, 16, 0, 16, 8, p, None, p + 2, None, 1, p, None) == ERR_ARG
+    # sizes beyond the fixed scratch
+    assert L.shkz_b200_conv3d_noalloc(16, 16, 16, 16, 0, 256, 4, p, None, p, None, 1, p, None) == ERR_LIMIT
+    assert L.shkz_b200_conv3d_noalloc(16, 16, 16, 128, 16, 16, 8, p, p, p, None, 1, p, None) == ERR_LIMIT
