@@ -83,7 +83,15 @@ typedef struct shkz_b200_config {
   int warm_start;             /* WarmStart (default 0) */
   int index_tile;             /* tile edge of the caller's grids (TileSize, default 16): unknown numbering of
                                  the warm-start vector */
-  int reserved[4];
+  int spin_limit;             /* polling rounds of every bounded device wait (tile faces and flags of the MIC(0)
+                                 wavefronts) before it gives up and the call returns SHKZ_B200_ERR_TIMEOUT;
+                                 0 = the default, 2^21 (about 0.15 s) */
+  int fault_skip_publish;     /* fault injection, 0 = off: k > 0 makes the forward MIC(0) sweep's k-th wavefront
+                                 slot skip publishing its faces, so its consumers' bounded waits run out */
+  int device_mem_limit_mb;    /* cap on the device memory of the context's grid and tile-pool buffers, in MiB;
+                                 a call that would exceed it returns SHKZ_B200_ERR_NOMEM (0 = no cap) */
+  int csr_preconditioner;     /* shkz_b200_solve_csr: SHKZ_B200_PRECOND_NONE (default: what the shipped pcg
+                                 runs) or SHKZ_B200_PRECOND_MIC0 (the header's MIC(0) applied) */
 } shkz_b200_config;
 
 /* Fill *cfg with the defaults listed above. */
@@ -139,7 +147,15 @@ typedef struct shkz_b200_result {
   double ms_h2d, ms_d2h;     /* host paths only */
   long long kernel_launches; /* CUDA kernels this library launched for the call */
   double volume_rhs_correct; /* volume correction added to every rhs row (record _volume_correct_rhs), else 0 */
-  double reserved[6];
+  /* sub-phases of ms_assemble, under the reference's record names
+   * (macpressuresolver3.cpp:95,168,218): face fractions and the unknown mask
+   * (one kernel; solid_fluid_fractions), the unknown numbering by tile-pool
+   * compaction (labelling_cells), the system's weights and rhs
+   * (build_highres_linsystem, with the volume correction inside) */
+  double ms_fractions;
+  double ms_labelling;
+  double ms_build;
+  double reserved[3];
 } shkz_b200_result;
 
 /* macproject3_interface::set_target_volume (macpressuresolver3.cpp:46-49):
@@ -255,14 +271,27 @@ int shkz_b200_splat_device(shkz_b200_ctx *ctx, const shkz_b200_splat_args *args)
  * can order their own work against it. */
 void *shkz_b200_stream(shkz_b200_ctx *ctx);
 
+/* Page-locked host memory for the buffers of the host-buffer entry points:
+ * the host<->device copies of shkz_b200_project_host (and the other *_host
+ * calls) run at full link speed from it, where pageable memory is first
+ * copied through a bounce buffer by the CUDA driver. Returns NULL on failure;
+ * free with shkz_b200_host_free. No counterpart in the reference (its grids
+ * live in host memory only). */
+void *shkz_b200_host_alloc(size_t bytes);
+void shkz_b200_host_free(void *p);
+
 /* Generic solver path for LinSolver= (replaces pcg_solver::solve,
  * src/linsolver/pcg.cpp:45-73): solves A x = b for a symmetric CSR matrix
- * given on the host (row-sorted, 0-based, FP64) with the algorithm the
- * reference's pcg module runs as shipped -- conjugate gradients with the
- * identity preconditioner (its MIC(0) result is overwritten,
- * local/include/pcgsolver/pcg_solver.h:379-384), x0 = 0, stop at
- * ||r||inf <= residual * ||b||inf, iterations = iteration + 1 -- in FP64 on
- * the device. The config's preconditioner field is not used here. */
+ * given on the host (row-sorted, 0-based, FP64) with the reference's PCG loop
+ * (local/include/pcgsolver/pcg_solver.h:246-295), x0 = 0, stop at
+ * ||r||inf <= residual * ||b||inf, iterations = iteration + 1, in FP64 on the
+ * device. With csr_preconditioner = NONE (default) the preconditioner is the
+ * identity, which is what the shipped pcg module runs (its MIC(0) result is
+ * overwritten, pcg_solver.h:379-384); with MIC0 it is the header's own
+ * modified incomplete Cholesky (pcg_solver.h:88-223, mic_omega and
+ * mic_min_diag_ratio), factored and applied on the device over level
+ * schedules of the factor's pattern. The config's preconditioner field is
+ * not used here. */
 int shkz_b200_solve_csr(shkz_b200_ctx *ctx, long long n, const long long *indptr, const long long *indices,
                         const double *data, const double *b, double *x, shkz_b200_result *out);
 

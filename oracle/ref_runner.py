@@ -44,6 +44,7 @@ class RefResult:
     reresid: Optional[float] = None
     solve_ms: Optional[float] = None
     system: Optional[dict] = None
+    stdout: str = ""
 
 
 def _read_cells(f, shape_zyx):
@@ -113,7 +114,7 @@ def run_reference(scene, variant: str = "float", mode: str = "mic0", tol: Option
                         pressure=p, pressure_active=pm,
                         velocity=[v for v, _ in vout], velocity_active=[m for _, m in vout],
                         projection_ms=ms,
-                        console_solves=[(int(a), float(b)) for a, b in solves])
+                        console_solves=[(int(a), float(b)) for a, b in solves], stdout=proc.stdout)
         if dump_system and os.path.exists(dump + ".solve.txt"):
             it, rr, sms = open(dump + ".solve.txt").read().split()
             res.iterations, res.reresid, res.solve_ms = int(it), float(rr), float(sms)

@@ -32,8 +32,9 @@ UNITS = {
     "warmstart.cu": [],
     "extend.cu": ["-fmad=false"],
     "splat.cu": ["-fmad=false"],
+    "csr_mic0.cu": [],
 }
-HEADERS = ["common.cuh", "kernels.h", "solver.h", "learned.h", "tc_conv.cuh"]
+HEADERS = ["common.cuh", "kernels.h", "solver.h", "learned.h", "tc_conv.cuh", "csr_mic0.h"]
 
 
 def _stale(target: str, deps) -> bool:

@@ -12,6 +12,7 @@
 #include "kernels.h"
 #include "solver.h"
 #include "learned.h"
+#include "csr_mic0.h"
 #include "../../include/shkz_b200.h"
 
 #include <cmath>
@@ -19,6 +20,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 using namespace shkz;
@@ -34,7 +36,7 @@ struct shkz_b200_ctx {
   shkz_b200_config cfg;
   int device = 0;
   cudaStream_t stream = nullptr;
-  cudaEvent_t ev[8] = {};
+  cudaEvent_t ev[12] = {};
   // dense capacities
   size_t cap_cells = 0;
   size_t cap_h_cells = 0, cap_h_nodes = 0, cap_h_faces[3] = {0, 0, 0};
@@ -110,6 +112,8 @@ struct shkz_b200_ctx {
   size_t cap_sp_out[3] = {0, 0, 0};
   void *flush = nullptr;           // 256 MB written between timed kernel launches (> L2)
   size_t cap_h_dens[3] = {0, 0, 0};
+  std::unordered_map<void *, size_t> held;  // buffers allocated by grow() and their bytes
+  size_t held_bytes = 0;
 };
 
 extern "C" void shkz_b200_default_config(shkz_b200_config *c) {
@@ -152,26 +156,63 @@ extern "C" const char *shkz_b200_errstr(int code) {
 
 extern "C" const char *shkz_b200_last_error(shkz_b200_ctx *) { return g_last_error; }
 
+extern "C" void *shkz_b200_host_alloc(size_t bytes) {
+  void *p = nullptr;
+  if (!bytes) return nullptr;
+  const cudaError_t e = cudaMallocHost(&p, bytes);
+  if (e != cudaSuccess) {
+    shkz_set_cuda_error(e, "cudaMallocHost", __FILE__, __LINE__);
+    return nullptr;
+  }
+  return p;
+}
+
+extern "C" void shkz_b200_host_free(void *p) {
+  if (p) cudaFreeHost(p);
+}
+
+// Grid and tile-pool buffers of the context: freed and reallocated when a
+// call needs more. Their bytes are counted against cfg.device_mem_limit_mb
+// (when set), which refuses an allocation with SHKZ_B200_ERR_NOMEM before
+// cudaMalloc is asked.
+static void release(shkz_b200_ctx *ctx, void *p) {
+  if (!p) return;
+  auto it = ctx->held.find(p);
+  if (it != ctx->held.end()) {
+    ctx->held_bytes -= it->second;
+    ctx->held.erase(it);
+  }
+  cudaFree(p);
+}
+
 template <class T>
-static int grow(T **ptr, size_t need, size_t &cap_dummy) {
-  (void)cap_dummy;
-  if (*ptr) cudaFree(*ptr);
+static int grow(shkz_b200_ctx *ctx, T **ptr, size_t need, const char *what) {
+  release(ctx, *ptr);
   *ptr = nullptr;
   if (need == 0) return 0;
-  cudaError_t e = cudaMalloc((void **)ptr, need * sizeof(T));
+  const size_t bytes = need * sizeof(T);
+  const size_t cap = (size_t)(ctx->cfg.device_mem_limit_mb > 0 ? ctx->cfg.device_mem_limit_mb : 0) << 20;
+  if (cap && ctx->held_bytes + bytes > cap) {
+    std::snprintf(g_last_error, sizeof(g_last_error),
+                  "device memory cap of %d MiB reached: %zu bytes held, %zu more requested for %s",
+                  ctx->cfg.device_mem_limit_mb, ctx->held_bytes, bytes, what);
+    return SHKZ_B200_ERR_NOMEM;
+  }
+  cudaError_t e = cudaMalloc((void **)ptr, bytes);
   if (e != cudaSuccess) {
     shkz_set_cuda_error(e, "cudaMalloc", __FILE__, __LINE__);
     *ptr = nullptr;
     return SHKZ_B200_ERR_NOMEM;
   }
+  ctx->held[*ptr] = bytes;
+  ctx->held_bytes += bytes;
   return 0;
 }
 
-#define GROW(field, n)                                  \
-  do {                                                  \
-    size_t _d = 0;                                      \
-    int _rc = grow(&ctx->field, (size_t)(n), _d);       \
-    if (_rc) return _rc;                                \
+#define GROW(field, n)                                    \
+  do {                                                    \
+    int _rc = grow(ctx, &ctx->field, (size_t)(n), #field); \
+    if (_rc) return _rc;                                  \
   } while (0)
 
 static Geometry make_geometry(int nx, int ny, int nz) {
@@ -227,7 +268,7 @@ static int ensure_host_staging(shkz_b200_ctx *ctx, const Geometry &G, bool solid
     if (nf > ctx->cap_h_faces[d]) {
       GROW(h_vel[d], nf);
       GROW(h_vact[d], nf);
-      if (ctx->h_svel[d]) { cudaFree(ctx->h_svel[d]); ctx->h_svel[d] = nullptr; }
+      if (ctx->h_svel[d]) { release(ctx, ctx->h_svel[d]); ctx->h_svel[d] = nullptr; }
       ctx->cap_h_faces[d] = nf;
     }
     if (svel[d] && !ctx->h_svel[d]) GROW(h_svel[d], ctx->cap_h_faces[d]);
@@ -416,6 +457,21 @@ static PoolSystem pool_system(shkz_b200_ctx *ctx) {
 
 static char *wsync(shkz_b200_ctx *ctx, int which) { return (char *)ctx->ws + which * wave_sync_bytes(); }
 
+// Before a call's wavefront kernels: clear the three wave-sync error words
+// (a timed-out call leaves one set) and write the configured spin limit and
+// the fault-injection slot (forward sweep only). The words are
+// error, spin_limit, skip_publish at byte offset 12 of each WaveSync; the
+// slot, epoch and finished words are left alone, so face tags stay valid.
+static int arm_waves(shkz_b200_ctx *ctx) {
+  for (int w = 0; w < 3; ++w) {
+    const int words[3] = {0, ctx->cfg.spin_limit > 0 ? ctx->cfg.spin_limit : 0,
+                          w == 1 && ctx->cfg.fault_skip_publish > 0 ? ctx->cfg.fault_skip_publish : 0};
+    SHKZ_CUDA_TRY(cudaMemcpyAsync(wsync(ctx, w) + 3 * sizeof(int), words, sizeof(words), cudaMemcpyHostToDevice,
+                                  ctx->stream));
+  }
+  return 0;
+}
+
 // Wave-sync error word (offset of `error` inside WaveSync is 3 ints).
 static int wave_errors(shkz_b200_ctx *ctx) {
   std::vector<char> h(3 * wave_sync_bytes());
@@ -521,6 +577,8 @@ static int solve_system(shkz_b200_ctx *ctx, double tol, int precond, shkz_b200_r
     }
     SHKZ_CUDA_TRY(cudaMemcpyAsync(&hst, ctx->st, sizeof(hst), cudaMemcpyDeviceToHost, s));
     SHKZ_CUDA_TRY(cudaStreamSynchronize(s));
+    // a bounded wait that gave up leaves its iterate undefined: stop here
+    if (wave_errors(ctx)) { rc = SHKZ_B200_ERR_TIMEOUT; break; }
     if (hst.done == 0) continue;
     if (hst.done == 3 || hst.status == -5) { rc = SHKZ_B200_ERR_NAN; break; }
     if (hst.done == 2) break;
@@ -695,6 +753,9 @@ static int ensure_warm(shkz_b200_ctx *ctx, const Geometry &G, int T, long long u
 static int project_device(shkz_b200_ctx *ctx, const shkz_b200_project_args *a, shkz_b200_result *res) {
   cudaStream_t s = ctx->stream;
   const Geometry G = make_geometry(a->nx, a->ny, a->nz);
+  // the previous system's buffers may be regrown (or fail to be) below:
+  // nothing may inspect or reuse that system until this call completes one
+  ctx->has_system = 0;
   int rc = ensure_grid(ctx, G);
   if (rc) return rc;
   AssemblyInputs in;
@@ -720,6 +781,7 @@ static int project_device(shkz_b200_ctx *ctx, const shkz_b200_project_args *a, s
   const long long launches0 = launches_so_far();
   cudaEventRecord(ctx->ev[0], s);
   launch_label(in, ctx->flags, ctx->unk, ctx->tile_count, s);
+  cudaEventRecord(ctx->ev[8], s);
   if (a->surface_tension != 0.0) {
     // velocity += surface tension force before the system is built (it reads the new velocity)
     const size_t cells = (size_t)G.nx * G.ny * G.nz;
@@ -744,6 +806,9 @@ static int project_device(shkz_b200_ctx *ctx, const shkz_b200_project_args *a, s
   SHKZ_CUDA_TRY(cudaGetLastError());
   rc = build_macro_tiles(ctx, G, K, s);
   if (rc) return rc;
+  rc = arm_waves(ctx);
+  if (rc) return rc;
+  cudaEventRecord(ctx->ev[9], s);
   ctx->K = K;
   ctx->G = G;
   ctx->model_ready = 0;
@@ -763,6 +828,7 @@ static int project_device(shkz_b200_ctx *ctx, const shkz_b200_project_args *a, s
   CoeffOutputs co{ctx->diag, ctx->offx, ctx->offy, ctx->offz, ctx->diag64, ctx->offx64, ctx->offy64, ctx->offz64,
                   ctx->rhs64};
   launch_coeff(in, ctx->flags, ctx->pool_tile, K, ctx->unk, co, s);
+  cudaEventRecord(ctx->ev[10], s);
   const bool warm = K > 0 && ctx->cfg.warm_start;
   if (warm) {
     // b <- b - A x_prev with x_prev read by the reference's unknown number
@@ -835,6 +901,9 @@ static int project_device(shkz_b200_ctx *ctx, const shkz_b200_project_args *a, s
   res->ms_solve = ms_between(ctx->ev[1], ctx->ev[2]);
   res->ms_update = ms_between(ctx->ev[2], ctx->ev[3]);
   res->ms_total = ms_between(ctx->ev[0], ctx->ev[3]);
+  res->ms_fractions = ms_between(ctx->ev[0], ctx->ev[8]);
+  res->ms_labelling = ms_between(ctx->ev[8], ctx->ev[9]);
+  res->ms_build = ms_between(ctx->ev[9], ctx->ev[10]);
   res->kernel_launches = launches_so_far() - launches0;
   res->status = solve_rc;
   return solve_rc;
@@ -1312,6 +1381,8 @@ static int dense_roundtrip(shkz_b200_ctx *ctx, const float *in_cells, float *out
   const size_t cells = (size_t)G.nx * G.ny * G.nz;
   const int n = ctx->K * SHKZ_TC;
   float *dense = nullptr;
+  int rc = arm_waves(ctx);
+  if (rc) return rc;
   SHKZ_CUDA_TRY(cudaMalloc(&dense, cells * 4));
   cudaMemcpyAsync(dense, in_cells, cells * 4, cudaMemcpyHostToDevice, s);
   if (ctx->K > 0) {
@@ -1372,6 +1443,8 @@ extern "C" int shkz_b200_solve_csr(shkz_b200_ctx *ctx, long long n, const long l
   if (n == 0) return 0;
   const long long nnz = indptr[n];
   if (n > INT32_MAX || nnz > INT32_MAX) return res->status = SHKZ_B200_ERR_LIMIT;
+  const bool mic = ctx->cfg.csr_preconditioner == SHKZ_B200_PRECOND_MIC0;
+  if (!mic && ctx->cfg.csr_preconditioner != SHKZ_B200_PRECOND_NONE) return res->status = SHKZ_B200_ERR_ARG;
   cudaSetDevice(ctx->device);
   cudaStream_t s = ctx->stream;
   std::vector<int> hp((size_t)n + 1), hi((size_t)nnz);
@@ -1385,28 +1458,46 @@ extern "C" int shkz_b200_solve_csr(shkz_b200_ctx *ctx, long long n, const long l
     if (dd) cudaFree(dd);
     if (vb) cudaFree(vb);
   };
-  // vectors: r, x, s(p), z(q) and reduction scratch
+  // vectors: r, x, s(p), z(q), the preconditioned residual and reduction scratch
   if (cudaMalloc(&dp, sizeof(int) * (n + 1)) != cudaSuccess || cudaMalloc(&di, sizeof(int) * (nnz ? nnz : 1)) != cudaSuccess ||
       cudaMalloc(&dd, sizeof(double) * (nnz ? nnz : 1)) != cudaSuccess ||
-      cudaMalloc(&vb, sizeof(double) * (4 * (size_t)n + 3 * 8192 + 8)) != cudaSuccess) {
+      cudaMalloc(&vb, sizeof(double) * (5 * (size_t)n + 3 * 8192 + 8)) != cudaSuccess) {
     cleanup();
     return res->status = SHKZ_B200_ERR_NOMEM;
   }
-  double *r = vb, *xv = vb + n, *p = vb + 2 * n, *q = vb + 3 * n, *part = vb + 4 * n, *out = part + 3 * 8192;
+  double *r = vb, *xv = vb + n, *p = vb + 2 * n, *q = vb + 3 * n, *zv = vb + 4 * n, *part = vb + 5 * n,
+         *out = part + 3 * 8192;
   unsigned *cnt = ctx->counter + 4;
   cudaMemcpyAsync(dp, hp.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, s);
   cudaMemcpyAsync(di, hi.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice, s);
   cudaMemcpyAsync(dd, data, sizeof(double) * nnz, cudaMemcpyHostToDevice, s);
   cudaMemcpyAsync(r, b, sizeof(double) * n, cudaMemcpyHostToDevice, s);
   cudaMemsetAsync(xv, 0, sizeof(double) * n, s);
+  CsrMic0 M;
+  if (mic) {
+    int rc = M.build((int)n, hp.data(), hi.data(), dp, di, s);
+    if (!rc) rc = M.factor(dd, ctx->cfg.mic_omega, ctx->cfg.mic_min_diag_ratio, s);
+    if (rc) {
+      cleanup();
+      return res->status = rc;
+    }
+  }
   double h[3];
-  auto dots = [&](const double *a, const double *bb) -> bool {
-    launch_dots64((int)n, a, bb, nullptr, nullptr, part, cnt, out, s);
+  // out = {a.b, c.d, max|a|}
+  auto dots = [&](const double *a, const double *bb, const double *c, const double *d) -> bool {
+    launch_dots64((int)n, a, bb, c, d, part, cnt, out, s);
     return cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, s) == cudaSuccess &&
            cudaStreamSynchronize(s) == cudaSuccess;
   };
+  // z = M^-1 r (pcg_solver.h:378-385 with the MIC(0) result kept), or z = r
+  auto precondition = [&]() -> const double * {
+    if (!mic) return r;
+    M.apply(r, zv, s);
+    return zv;
+  };
   int rc = 0, it = 0;
-  if (!dots(r, r)) { cleanup(); return res->status = SHKZ_B200_ERR_CUDA; }
+  const double *z = precondition();
+  if (!dots(r, r, z, r)) { cleanup(); return res->status = SHKZ_B200_ERR_CUDA; }
   const double r0 = h[2];
   double rmax = r0;
   if (r0 == 0.0) {
@@ -1414,21 +1505,22 @@ extern "C" int shkz_b200_solve_csr(shkz_b200_ctx *ctx, long long n, const long l
     res->reresid = 0.0;
   } else {
     const double tol = ctx->cfg.residual * r0;
-    double rho = h[0];
-    cudaMemcpyAsync(p, r, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
+    double rho = h[1];
+    cudaMemcpyAsync(p, z, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
     const int grid = (int)std::min<long long>((n + 255) / 256, 148 * 16);
     for (it = 0; it < ctx->cfg.max_iterations; ++it) {
       count_launches(1);
       k_csr_spmv64<<<grid, 256, 0, s>>>((int)n, dp, di, dd, p, q);
-      if (!dots(p, q)) { rc = SHKZ_B200_ERR_CUDA; break; }
+      if (!dots(p, q, nullptr, nullptr)) { rc = SHKZ_B200_ERR_CUDA; break; }
       const double alpha = rho / h[0];
       launch_axpy2_64((int)n, alpha, p, xv, q, r, s);
-      if (!dots(r, r)) { rc = SHKZ_B200_ERR_CUDA; break; }
+      z = precondition();
+      if (!dots(r, r, z, r)) { rc = SHKZ_B200_ERR_CUDA; break; }
       rmax = h[2];
       if (!(rmax == rmax)) { rc = SHKZ_B200_ERR_NAN; break; }
       if (rmax <= tol) { ++it; break; }
-      const double rho_new = h[0];
-      launch_xpby64((int)n, r, rho_new / rho, p, s);
+      const double rho_new = h[1];
+      launch_xpby64((int)n, z, rho_new / rho, p, s);
       rho = rho_new;
     }
     res->iterations = it;
@@ -1439,6 +1531,7 @@ extern "C" int shkz_b200_solve_csr(shkz_b200_ctx *ctx, long long n, const long l
     rc = SHKZ_B200_ERR_CUDA;
   cleanup();
   res->unknowns = n;
+  res->outer_steps = mic ? M.levels() : 0;
   res->status = rc;
   return rc;
 }
@@ -1458,6 +1551,8 @@ extern "C" int shkz_b200_time_kernel(shkz_b200_ctx *ctx, int which, int reps, do
   init.alpha = 1e-30;  // keeps x and r unchanged to rounding while timing the update
   init.beta = 0.0;
   init.tol_abs = -1.0;
+  const int arm = arm_waves(ctx);
+  if (arm) return arm;
   SHKZ_CUDA_TRY(cudaMemcpyAsync(ctx->st_scratch, &init, sizeof(init), cudaMemcpyHostToDevice, s));
   auto launch = [&]() {
     switch (which) {
@@ -1609,6 +1704,7 @@ static int learned_solve(shkz_b200_ctx *ctx, double tol, shkz_b200_result *res) 
     launch_update_xr(n, ctx->p, ctx->q, ctx->x, ctx->r, ctx->partials, ctx->counter + 1, ctx->st, max_it, s);
     SHKZ_CUDA_TRY(cudaMemcpyAsync(&hst, ctx->st, sizeof(hst), cudaMemcpyDeviceToHost, s));
     SHKZ_CUDA_TRY(cudaStreamSynchronize(s));
+    if (use_mic && wave_errors(ctx)) { rc = SHKZ_B200_ERR_TIMEOUT; break; }
     if (hst.done == 5) {
       // the learned z broke down (z.r <= 0 or not finite): x and r are those of
       // the last completed iteration; continue with MIC(0) from r

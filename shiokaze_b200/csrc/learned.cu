@@ -14,9 +14,9 @@
 // Activations are dense channels-last BF16 tensors per level, zero outside
 // the active 8x16x8 blocks (blocks that touch a tile of the solver's pool).
 // Every 3^3 convolution (forward, and the input gradient with flipped and
-// transposed weights) runs on the tcgen05 implicit-GEMM kernel of tc_conv.cuh.
-// Weight gradients are FP32 reductions on the CUDA cores; Adam keeps FP32
-// master weights and moments.
+// transposed weights) runs on the tcgen05 implicit-GEMM kernel of tc_conv.cuh;
+// weight gradients run on tcgen05 too (k_wgrad_tc, voxels as the reduction
+// dimension). Adam keeps FP32 master weights and moments.
 #include "common.cuh"
 #include "kernels.h"
 #include "learned.h"
@@ -492,94 +492,173 @@ __global__ void k_pool_grad(const float *Gc, int C, int hx, int hy, int hz, cons
   }
 }
 
-// Weight gradient dW[t][co][ci] += sum_v gpre[v][co] * X(v + off_t)[ci] and
-// bias gradient, FP32 on the CUDA cores. One CTA (256 threads) per active
-// block and 16-channel input chunk; the block's gpre and the chunk's halo are
-// staged in shared memory; each thread accumulates a 4 (co) x 4 (ci) tile of
-// one tap over the block's voxels, then adds it to dW with atomics.
-__global__ void __launch_bounds__(256) k_wgrad(const __nv_bfloat16 *gpre, int cout_pad, int cout_real,
-                                               const __nv_bfloat16 *in0, int c0, const __nv_bfloat16 *in1, int c1,
-                                               int nx, int ny, int nz, int hx, int hy, int hz, const uint8_t *blk,
-                                               int gbx, int gby, int gbz, float *dW, float *db) {
-  extern __shared__ __align__(16) uint8_t sm[];
-  __nv_bfloat16 *G = reinterpret_cast<__nv_bfloat16 *>(sm);                    // [8][16][8][cout_pad]
-  __nv_bfloat16 *H = G + 1024 * cout_pad;                                      // [10][18][10][16]
+// Weight gradient on the tensor cores (tcgen05, kind::f16, M = 64, N = 16,
+// K = voxels): for one active block (8 x 16 x 8 voxels) and one 16-channel
+// input chunk,
+//   D_t[co][ci] = sum_v gpre[v][co] * X(v + off_t)[ci]      for the 27 taps t,
+// accumulated in TMEM (tap t in columns 16 t .. 16 t + 15) over four
+// sub-blocks of two z planes (256 voxels). Both operands are MN-major, so the
+// staged data keep their channels-last order:
+//   A = gpre: 8-channel groups g of 256 voxels x 16 B, byte g * 4096 + k * 16
+//       (k = x + 8 y + 128 z); SBO = 4096 B between channel groups, LBO = 128 B
+//       between the 8-voxel groups of a K step;
+//   B = the input halo of the sub-block, (4 z) x 18 x 10 voxels x 16 B per
+//       8-channel half, the canonical layout of the forward kernel; a tap is
+//       the same layout shifted, so only the start address changes; SBO = the
+//       half's size between the channel halves, LBO = 160 B (one y row)
+//       between the 8-voxel groups of a K step.
+// The next sub-block is staged (cp.async) while the tensor cores work on the
+// current one. Row co of D sits in TMEM lane (co % 16) + 32 (co / 16), so warp
+// w reads output channels 16 w .. 16 w + 15 in its first 16 lanes, adds them
+// to dW with atomics, and the bias gradient is summed from the staged gpre.
+__global__ void __launch_bounds__(128, 1) k_wgrad_tc(const __nv_bfloat16 *gpre, int cout_pad, int cout_real,
+                                                     const __nv_bfloat16 *in0, int c0, const __nv_bfloat16 *in1,
+                                                     int c1, int nx, int ny, int nz, int hx, int hy, int hz,
+                                                     const uint8_t *blk, int gbx, int gby, int gbz, float *dW,
+                                                     float *db, int *err) {
+  constexpr uint32_t kG = 8 * 256 * 16;        // staged gpre of a sub-block
+  constexpr uint32_t kHH = 4 * 18 * 10 * 16;   // one 8-channel half of the halo
+  constexpr uint32_t kBuf = kG + 2 * kHH;      // one stage (55,808 bytes)
+  extern __shared__ __align__(1024) uint8_t smem[];
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + 2 * kBuf);
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mbar + 1);
   const int cin = c0 + c1;
   const int nchunk = cin / 16;
   int bid = blockIdx.x;
   const int chunk = bid % nchunk;
   bid /= nchunk;
   const int bxi = bid % gbx, byi = (bid / gbx) % gby, bzi = bid / (gbx * gby);
-  if (!blk[((size_t)bzi * gby + byi) * gbx + bxi]) return;
+  if (!blk[((size_t)bzi * gby + byi) * gbx + bxi]) return;  // whole CTA
   const int X0 = bxi * 8, Y0 = byi * 16, Z0 = bzi * 8;
-  const int tid = threadIdx.x;
-  for (int e = tid; e < 1024 * cout_pad / 8; e += 256) {
-    const int v = (e * 8) / cout_pad, c = (e * 8) % cout_pad;
-    const int x = v & 7, y = (v >> 3) & 15, z = v >> 7;
-    const int X = X0 + x, Y = Y0 + y, Z = Z0 + z;
-    uint4 val = make_uint4(0, 0, 0, 0);
-    if (X < nx && Y < ny && Z < nz) val = *reinterpret_cast<const uint4 *>(gpre + (((size_t)Z * ny + Y) * nx + X) * cout_pad + c);
-    *reinterpret_cast<uint4 *>(G + (size_t)v * cout_pad + c) = val;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t s0 = smem_u32(smem), bar_s = smem_u32(mbar);
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(512)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
-  for (int e = tid; e < 1800 * 2; e += 256) {
-    const int v = e >> 1, kh = e & 1;
-    const int xx = v % 10, yy = (v / 10) % 18, zz = v / 180;
-    const int X = X0 + xx - 1, Y = Y0 + yy - 1, Z = Z0 + zz - 1;
-    const int c = chunk * 16 + kh * 8;
-    uint4 val = make_uint4(0, 0, 0, 0);
-    if (X >= 0 && Y >= 0 && Z >= 0 && X < nx && Y < ny && Z < nz) {
-      if (c < c0) val = *reinterpret_cast<const uint4 *>(in0 + (((size_t)Z * ny + Y) * nx + X) * c0 + c);
-      else {
-        const int hX = X >> 1, hY = Y >> 1, hZ = Z >> 1;
-        if (hX < hx && hY < hy && hZ < hz)
-          val = *reinterpret_cast<const uint4 *>(in1 + (((size_t)hZ * hy + hY) * hx + hX) * c1 + (c - c0));
-      }
-    }
-    *reinterpret_cast<uint4 *>(H + (size_t)v * 16 + kh * 8) = val;
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_s) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  // tasks: (tap, co4, ci4): 27 * (cout_real padded to 4)/4 * 4
-  const int nco4 = (cout_real + 3) / 4;
-  const int ntask = 27 * nco4 * 4;
-  for (int task = tid; task < ntask; task += 256) {
-    const int ci4 = task & 3;
-    const int co4 = (task >> 2) % nco4;
-    const int t = (task >> 2) / nco4;
-    const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
-    float acc[4][4] = {};
-    for (int v = 0; v < 1024; ++v) {
-      const int x = v & 7, y = (v >> 3) & 15, z = v >> 7;
-      const __nv_bfloat16 *gp = G + (size_t)v * cout_pad + co4 * 4;
-      const __nv_bfloat16 *hp = H + (size_t)(((z + 1 + dz) * 18 + (y + 1 + dy)) * 10 + (x + 1 + dx)) * 16 + ci4 * 4;
-      float gv[4], hv[4];
-      #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        gv[i] = (co4 * 4 + i < cout_pad) ? __bfloat162float(gp[i]) : 0.f;
-        hv[i] = __bfloat162float(hp[i]);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+  // D FP32, A/B BF16, both MN-major, N = 16, M = 64
+  const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) | ((uint32_t)(16 >> 3) << 17) |
+                         ((uint32_t)(64 >> 4) << 24);
+  auto stage = [&](int sb, uint32_t buf) {
+    for (int e = tid; e < 2048; e += 128) {
+      const int g = e >> 8, k = e & 255;
+      const int X = X0 + (k & 7), Y = Y0 + ((k >> 3) & 15), Z = Z0 + 2 * sb + (k >> 7);
+      const bool in = 8 * g < cout_pad && X < nx && Y < ny && Z < nz;
+      const __nv_bfloat16 *src = in ? gpre + (((size_t)Z * ny + Y) * nx + X) * cout_pad + 8 * g : gpre;
+      cp_async16(buf + (uint32_t)(g * 4096 + k * 16), src, in ? 16 : 0);
+    }
+    for (int e = tid; e < 1440; e += 128) {
+      const int kh = e / 720, r = e % 720, zz = r / 180, yy = (r % 180) / 10, xx = r % 10;
+      const int X = X0 + xx - 1, Y = Y0 + yy - 1, Z = Z0 + 2 * sb + zz - 1;
+      const int c = chunk * 16 + kh * 8;
+      const __nv_bfloat16 *src = in0;
+      int bytes = 0;
+      if (X >= 0 && Y >= 0 && Z >= 0 && X < nx && Y < ny && Z < nz) {
+        if (c < c0) {
+          src = in0 + (((size_t)Z * ny + Y) * nx + X) * c0 + c;
+          bytes = 16;
+        } else {
+          const int hX = X >> 1, hY = Y >> 1, hZ = Z >> 1;
+          if (hX < hx && hY < hy && hZ < hz) {
+            src = in1 + (((size_t)hZ * hy + hY) * hx + hX) * c1 + (c - c0);
+            bytes = 16;
+          }
+        }
       }
-      #pragma unroll
-      for (int i = 0; i < 4; ++i)
+      cp_async16(buf + kG + (uint32_t)kh * kHH + (uint32_t)((zz * 18 + yy) * 10 + xx) * 16, src, bytes);
+    }
+  };
+  bool ok = true;
+  float bsum = 0.0f;
+  const bool bias = chunk == 0 && db != nullptr;
+  stage(0, s0);
+  cp_async_wait_all();
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  __syncthreads();
+  for (int sb = 0; sb < 4; ++sb) {
+    const uint32_t buf = s0 + (uint32_t)(sb & 1) * kBuf;
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      for (int t = 0; t < 27; ++t) {
+        const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
+        #pragma unroll 4
+        for (int j = 0; j < 16; ++j) {
+          const int y0 = (2 * j) & 15, zl = j >> 3;
+          const uint64_t da = umma_desc(buf + 256u * (uint32_t)j, 128, 4096);
+          const uint64_t dbd =
+              umma_desc(buf + kG + (uint32_t)(((zl + dz) * 18 + (y0 + dy)) * 10 + dx) * 16, 160, kHH);
+          const uint32_t acc = (sb > 0 || j > 0) ? 1u : 0u;
+          asm volatile(
+              "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+              "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem + (uint32_t)(t * 16)),
+              "l"(da), "l"(dbd), "r"(idesc), "r"(acc)
+              : "memory");
+        }
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar_s)
+                   : "memory");
+    }
+    __syncwarp();
+    // the next sub-block into the other stage while the tensor cores read this one
+    if (sb + 1 < 4) stage(sb + 1, s0 + (uint32_t)((sb + 1) & 1) * kBuf);
+    if (bias) {
+      // bias gradient: thread (co, half) sums half of the sub-block's voxels
+      const int co = tid & 63, half = tid >> 6;
+      if (co < cout_pad) {
+        const __nv_bfloat16 *G = reinterpret_cast<const __nv_bfloat16 *>(smem + (sb & 1) * kBuf);
+        for (int k = half * 128; k < half * 128 + 128; ++k) bsum += __bfloat162float(G[(co >> 3) * 2048 + k * 8 + (co & 7)]);
+      }
+    }
+    if (!mbar_wait(bar_s, (uint32_t)(sb & 1))) {
+      ok = false;
+      break;
+    }
+    cp_async_wait_all();
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (ok) {
+    const int co = 16 * warp + (lane & 15);
+    for (int t = 0; t < 27; ++t) {
+      uint32_t r[16];
+      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(t * 16);
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+          : "r"(taddr)
+          : "memory");
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (lane < 16 && co < cout_real) {
+        float *dst = dW + ((size_t)t * cout_real + co) * cin + chunk * 16;
         #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] += gv[i] * hv[j];
-    }
-    #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int co = co4 * 4 + i;
-      if (co >= cout_real) continue;
-      #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int ci = chunk * 16 + ci4 * 4 + j;
-        atomicAdd(&dW[((size_t)t * cout_real + co) * cin + ci], acc[i][j]);
+        for (int i = 0; i < 16; ++i) atomicAdd(dst + i, __uint_as_float(r[i]));
       }
     }
+    if (bias && (tid & 63) < cout_real) atomicAdd(&db[tid & 63], bsum);
+  } else {
+    if (tid == 0) atomicExch(err, 1);
+    // a bounded chance for the outstanding MMAs and copies to finish before
+    // TMEM and shared memory are released
+    mbar_wait(bar_s, 0);
+    mbar_wait(bar_s, 1);
+    cp_async_wait_all();
   }
-  if (chunk == 0 && db) {
-    for (int co = tid; co < cout_real; co += 256) {
-      float s = 0.f;
-      for (int v = 0; v < 1024; ++v) s += __bfloat162float(G[(size_t)v * cout_pad + co]);
-      atomicAdd(&db[co], s);
-    }
-  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
 }
 
 __global__ void k_adam(float *w, const float *g, float *m, float *v, int n, float lr, float b1, float b2, float eps,
@@ -974,17 +1053,20 @@ static int backward(LearnedModel *m, cudaStream_t s) {
           m->Gt[D.out], m->T[D.out], P.cout, P.n_pad, D.relu, nv, m->NX[lv], m->NY[lv], m->blk[lv], m->gb[lv][0],
           m->gb[lv][1], m->gpre);
     }
-    // weight and bias gradients
+    // weight and bias gradients on the tensor cores (one CTA per SM: it holds
+    // all 512 TMEM columns, and its 120 KB of shared memory keeps a second
+    // CTA from waiting in the allocation)
     {
       const int cin = D.c0 + D.c1;
-      const size_t smem = (size_t)1024 * P.n_pad * 2 + (size_t)1800 * 16 * 2;
-      cudaFuncSetAttribute(k_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+      const size_t smem = 120 * 1024;
+      cudaFuncSetAttribute(k_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       const int nb = m->gb[lv][0] * m->gb[lv][1] * m->gb[lv][2] * (cin / 16);
       count_launches(1);
-      k_wgrad<<<nb, 256, smem, s>>>(m->gpre, P.n_pad, P.cout, m->T[D.in0], D.c0, D.in1 >= 0 ? m->T[D.in1] : nullptr,
-                                    D.c1, m->NX[lv], m->NY[lv], m->NZ[lv], lv < 2 ? m->NX[lv + 1] : 0,
-                                    lv < 2 ? m->NY[lv + 1] : 0, lv < 2 ? m->NZ[lv + 1] : 0, m->blk[lv],
-                                    m->gb[lv][0], m->gb[lv][1], m->gb[lv][2], P.gw, P.gb);
+      k_wgrad_tc<<<nb, 128, smem, s>>>(m->gpre, P.n_pad, P.cout, m->T[D.in0], D.c0,
+                                       D.in1 >= 0 ? m->T[D.in1] : nullptr, D.c1, m->NX[lv], m->NY[lv], m->NZ[lv],
+                                       lv < 2 ? m->NX[lv + 1] : 0, lv < 2 ? m->NY[lv + 1] : 0,
+                                       lv < 2 ? m->NZ[lv + 1] : 0, m->blk[lv], m->gb[lv][0], m->gb[lv][1],
+                                       m->gb[lv][2], P.gw, P.gb, m->err);
     }
     if (li == 0) break;  // no input gradient needed for the first layer
     // input gradient: conv of gpre with the flipped, transposed weights

@@ -480,8 +480,16 @@ struct WaveSync {
   int slot;
   unsigned finished;
   int epoch;
-  int error;      // 0, or the slot that gave up waiting + 1
+  int error;         // 0, or the slot that gave up waiting + 1
+  int spin_limit;    // polling rounds of a bounded wait (0: SPIN_LIMIT); set by the host
+  int skip_publish;  // fault injection (0: off): wavefront slot k - 1 of a forward macro sweep does not publish
 };
+
+// Rounds a bounded wait polls before it gives up.
+__device__ __forceinline__ int spin_rounds(const WaveSync *ws) {
+  const int v = *((volatile const int *)&ws->spin_limit);
+  return v > 0 ? v : SPIN_LIMIT;
+}
 
 __device__ __forceinline__ int ld_acquire(const int *p) {
   int v;
@@ -493,8 +501,8 @@ __device__ __forceinline__ void st_release(int *p, int v) {
 }
 
 // Bounded wait for flag >= target. Returns false when the limit was hit.
-__device__ __forceinline__ bool wait_flag(const int *flag, int target) {
-  for (int it = 0; it < SPIN_LIMIT; ++it) {
+__device__ __forceinline__ bool wait_flag(const int *flag, int target, int limit) {
+  for (int it = 0; it < limit; ++it) {
     if (ld_acquire(flag) >= target) return true;
     if (it > 64) __nanosleep(64);
   }
@@ -534,9 +542,10 @@ __device__ __forceinline__ void wave_end(WaveSync *ws, int *flags, int pt, int t
 __device__ __forceinline__ void wave_wait(WaveSync *ws, const int *flags, const int *nb3, int target, int slot) {
   if (threadIdx.x == 0) {
     bool ok = true;
+    const int limit = spin_rounds(ws);
     #pragma unroll
     for (int i = 0; i < 3; ++i)
-      if (nb3[i] >= 0 && ok) ok = wait_flag(&flags[nb3[i]], target);
+      if (nb3[i] >= 0 && ok) ok = wait_flag(&flags[nb3[i]], target, limit);
     if (!ok) atomicCAS(&ws->error, 0, slot + 1);
   }
   // consumer side: thread 0's acquire, then the barrier, orders the other
@@ -629,11 +638,11 @@ __device__ __forceinline__ void face_put(unsigned long long *e, int epoch, float
 // it checks any of them, so once the last face lands the thread sees it one
 // L2 round trip later, not one per face. e0/e1/e2 null: no neighbour (0).
 __device__ __forceinline__ void face_get3(const unsigned long long *e0, const unsigned long long *e1,
-                                          const unsigned long long *e2, int epoch, float &v0, float &v1, float &v2,
-                                          bool &ok) {
+                                          const unsigned long long *e2, int epoch, int limit, float &v0, float &v1,
+                                          float &v2, bool &ok) {
   bool r0 = !e0, r1 = !e1, r2 = !e2;
   v0 = v1 = v2 = 0.0f;
-  for (int it = 0; it < SPIN_LIMIT && !(r0 && r1 && r2); ++it) {
+  for (int it = 0; it < limit && !(r0 && r1 && r2); ++it) {
     unsigned long long w0 = 0ull, w1 = 0ull, w2 = 0ull;
     if (!r0) asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(w0) : "l"(e0) : "memory");
     if (!r1) asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(w1) : "l"(e1) : "memory");
@@ -646,15 +655,17 @@ __device__ __forceinline__ void face_get3(const unsigned long long *e0, const un
   if (!(r0 && r1 && r2)) ok = false;
 }
 
-__device__ __forceinline__ void sweep_begin(WaveSync *ws, int &slot, int &epoch) {
-  __shared__ int s_slot, s_epoch;
+__device__ __forceinline__ void sweep_begin(WaveSync *ws, int &slot, int &epoch, int &limit) {
+  __shared__ int s_slot, s_epoch, s_limit;
   if (threadIdx.x == 0) {
     s_slot = atomicAdd(&ws->slot, 1);
     s_epoch = *((volatile int *)&ws->epoch) + 1;
+    s_limit = spin_rounds(ws);
   }
   __syncthreads();
   slot = s_slot;
   epoch = s_epoch;
+  limit = s_limit;
 }
 
 __device__ __forceinline__ void sweep_end(WaveSync *ws, int epoch) {
@@ -677,8 +688,8 @@ __global__ void __launch_bounds__(64) k_mic_forward(PoolSystem S, const int *sch
   __shared__ __align__(16) float T[SHKZ_TC], R[SHKZ_TC], Dd[SHKZ_TC], WX[SHKZ_TC], WY[SHKZ_TC], WZ[SHKZ_TC];
   __shared__ float hx[64], hy[64], hz[64];
   if (st && st->done) return;
-  int slot, epoch;
-  sweep_begin(ws, slot, epoch);
+  int slot, epoch, limit;
+  sweep_begin(ws, slot, epoch, limit);
   const int pt = sched[slot];
   const int tid = threadIdx.x, jj = tid & 7, kk = tid >> 3;
   const size_t tb = (size_t)pt * SHKZ_TC;
@@ -692,7 +703,7 @@ __global__ void __launch_bounds__(64) k_mic_forward(PoolSystem S, const int *sch
     bool ok = true;
     face_get3(nxm >= 0 ? faces + ((size_t)nxm * 3 + 0) * 64 + tid : nullptr,
               nym >= 0 ? faces + ((size_t)nym * 3 + 1) * 64 + tid : nullptr,
-              nzm >= 0 ? faces + ((size_t)nzm * 3 + 2) * 64 + tid : nullptr, epoch, hx[tid], hy[tid], hz[tid], ok);
+              nzm >= 0 ? faces + ((size_t)nzm * 3 + 2) * 64 + tid : nullptr, epoch, limit, hx[tid], hy[tid], hz[tid], ok);
     if (!ok) atomicCAS(&ws->error, 0, slot + 1);
   }
   __syncthreads();
@@ -730,8 +741,8 @@ __global__ void __launch_bounds__(64) k_mic_backward(PoolSystem S, const int *sc
   __shared__ float hx[64], hy[64], hz[64], ux[64], uy[64], uz[64];
   __shared__ double red[2];
   if (st && st->done) return;
-  int slot, epoch;
-  sweep_begin(ws, slot, epoch);
+  int slot, epoch, limit;
+  sweep_begin(ws, slot, epoch, limit);
   const int pt = sched[S.K - 1 - slot];
   const int tid = threadIdx.x, jj = tid & 7, kk = tid >> 3;
   const size_t tb = (size_t)pt * SHKZ_TC;
@@ -750,7 +761,7 @@ __global__ void __launch_bounds__(64) k_mic_backward(PoolSystem S, const int *sc
     bool ok = true;
     face_get3(nxp >= 0 ? faces + ((size_t)nxp * 3 + 0) * 64 + tid : nullptr,
               nyp >= 0 ? faces + ((size_t)nyp * 3 + 1) * 64 + tid : nullptr,
-              nzp >= 0 ? faces + ((size_t)nzp * 3 + 2) * 64 + tid : nullptr, epoch, hx[tid], hy[tid], hz[tid], ok);
+              nzp >= 0 ? faces + ((size_t)nzp * 3 + 2) * 64 + tid : nullptr, epoch, limit, hx[tid], hy[tid], hz[tid], ok);
     if (!ok) atomicCAS(&ws->error, 0, slot + 1);
   }
   __syncthreads();
@@ -945,7 +956,7 @@ struct SweepUpdate {
   int max_iterations;
 };
 
-__global__ void __launch_bounds__(256) k_mic_forward16(PoolSystem S, const float *__restrict__ d32,
+__global__ void __launch_bounds__(256, 2) k_mic_forward16(PoolSystem S, const float *__restrict__ d32,
                                                        const float *__restrict__ r, float *__restrict__ t,
                                                        unsigned long long *faces, WaveSync *ws, const SolverState *st,
                                                        SweepUpdate fu) {
@@ -953,8 +964,8 @@ __global__ void __launch_bounds__(256) k_mic_forward16(PoolSystem S, const float
   float *Tg = smf, *R = Tg + MGC, *Dd = R + MTC, *WX = Dd + MTC, *WY = WX + MTC, *WZ = WY + MTC;
   __shared__ int sub[8];
   if (st && st->done) return;
-  int slot, epoch;
-  sweep_begin(ws, slot, epoch);
+  int slot, epoch, limit;
+  sweep_begin(ws, slot, epoch, limit);
   const int mt = S.msched[slot];
   const int tid = threadIdx.x, jj = tid & 15, kk = tid >> 4;
   if (tid < 8) sub[tid] = S.msub[mt * 8 + tid];
@@ -974,35 +985,50 @@ __global__ void __launch_bounds__(256) k_mic_forward16(PoolSystem S, const float
   } else {
     macro_load5(sub, r, d32, S.offx, S.offy, S.offz, R, Dd, WX, WY, WZ);
   }
+  __syncthreads();
+  // The thread's x-row in registers, rotated by its wavefront offset
+  // o = jj + kk: slot k holds cell (k - o) mod 16, so the cell of step s
+  // (x = s - o) sits in slot s mod 16, a constant of the unrolled step loop.
+  const int o = jj + kk;
+  float cd[MT], cr[MT], cx[MT], cy[MT], cz[MT];
   {
-    // upstream faces straight into the ghost layer (x = -1, y = -1, z = -1)
+    const int rb = MT * jj + MT * MT * kk;
+    #pragma unroll
+    for (int k = 0; k < MT; ++k) {
+      const int c = rb + ((k - o) & (MT - 1));
+      cd[k] = Dd[c]; cr[k] = R[c]; cx[k] = WX[c]; cy[k] = WY[c]; cz[k] = WZ[c];
+    }
+  }
+  float tx;
+  {
     const int nxm = S.mnbr[mt * 6 + NB_XM], nym = S.mnbr[mt * 6 + NB_YM], nzm = S.mnbr[mt * 6 + NB_ZM];
     const int u = tid & 15, v = tid >> 4;
     bool ok = true;
     float gx, gy, gz;
     face_get3(nxm >= 0 ? faces + ((size_t)nxm * 3 + 0) * 256 + tid : nullptr,
               nym >= 0 ? faces + ((size_t)nym * 3 + 1) * 256 + tid : nullptr,
-              nzm >= 0 ? faces + ((size_t)nzm * 3 + 2) * 256 + tid : nullptr, epoch, gx, gy, gz, ok);
+              nzm >= 0 ? faces + ((size_t)nzm * 3 + 2) * 256 + tid : nullptr, epoch, limit, gx, gy, gz, ok);
     Tg[mghost(-1, u, v)] = gx;
     Tg[mghost(u, -1, v)] = gy;
     Tg[mghost(u, v, -1)] = gz;
+    tx = gx;
     if (!ok) atomicCAS(&ws->error, 0, slot + 1);
   }
   __syncthreads();
   {
-    // cell ii = s - jj - kk of the thread's row: coefficient index s + cb,
-    // ghosted index s + gb; neighbour reads need no boundary test
-    const int cb = 15 * jj + 255 * kk, gb = mghost(0, jj, kk) - jj - kk;
+    const int gb = mghost(0, jj, kk) - o;
+    #pragma unroll
     for (int s = 0; s < 3 * MT - 2; ++s) {
-      if ((unsigned)(s - jj - kk) < (unsigned)MT) {
-        const int c = s + cb, g = s + gb;
-        const float tx = Tg[g - 1], ty = Tg[g - MGY], tz = Tg[g - MGZ];
-        Tg[g] = Dd[c] * (R[c] + WX[c] * tx + WY[c] * ty + WZ[c] * tz);
+      if ((unsigned)(s - o) < (unsigned)MT) {
+        const int g = s + gb, k = s & (MT - 1);
+        const float ty = Tg[g - MGY], tz = Tg[g - MGZ];
+        tx = cd[k] * (cr[k] + cx[k] * tx + cy[k] * ty + cz[k] * tz);
+        Tg[g] = tx;
       }
       __syncthreads();
     }
   }
-  {
+  if (*((volatile const int *)&ws->skip_publish) != slot + 1) {
     unsigned long long *f = faces + (size_t)mt * 3 * 256;
     const int u = tid & 15, v = tid >> 4;
     face_put(f + 0 * 256 + tid, epoch, Tg[mghost(15, u, v)]);
@@ -1036,7 +1062,7 @@ __global__ void __launch_bounds__(256) k_mic_forward16(PoolSystem S, const float
   sweep_end(ws, epoch);
 }
 
-__global__ void __launch_bounds__(256) k_mic_backward16(PoolSystem S, const float *__restrict__ d32,
+__global__ void __launch_bounds__(256, 2) k_mic_backward16(PoolSystem S, const float *__restrict__ d32,
                                                         const float *__restrict__ t, const float *__restrict__ r,
                                                         float *__restrict__ z, double *partials,
                                                         unsigned long long *faces, WaveSync *ws,
@@ -1046,8 +1072,8 @@ __global__ void __launch_bounds__(256) k_mic_backward16(PoolSystem S, const floa
   __shared__ int sub[8];
   __shared__ double red[8];
   if (st && st->done) return;
-  int slot, epoch;
-  sweep_begin(ws, slot, epoch);
+  int slot, epoch, limit;
+  sweep_begin(ws, slot, epoch, limit);
   const int mt = S.msched[S.KM - 1 - slot];
   const int tid = threadIdx.x, jj = tid & 15, kk = tid >> 4;
   if (tid < 8) sub[tid] = S.msub[mt * 8 + tid];
@@ -1107,28 +1133,43 @@ __global__ void __launch_bounds__(256) k_mic_backward16(PoolSystem S, const floa
       WZ[u + MT * v + MT * MT * (MT - 1)] = wzv;
     }
   }
+  __syncthreads();
+  // the thread's x-row in registers, rotated as in the forward sweep: slot k
+  // holds cell (k - o) mod 16
+  const int o = jj + kk;
+  float ct[MT], cd[MT], cx[MT], cy[MT], cz[MT];
   {
-    // downstream faces into the ghost layer (x = 16, y = 16, z = 16); the
-    // weight shifts above overlap the wait for them
+    const int rb = MT * jj + MT * MT * kk;
+    #pragma unroll
+    for (int k = 0; k < MT; ++k) {
+      const int c = rb + ((k - o) & (MT - 1));
+      ct[k] = Tt[c]; cd[k] = Dd[c]; cx[k] = WX[c]; cy[k] = WY[c]; cz[k] = WZ[c];
+    }
+  }
+  float zx;
+  {
     const int u = tid & 15, v = tid >> 4;
     bool ok = true;
     float gx, gy, gz;
     face_get3(nxp >= 0 ? faces + ((size_t)nxp * 3 + 0) * 256 + tid : nullptr,
               nyp >= 0 ? faces + ((size_t)nyp * 3 + 1) * 256 + tid : nullptr,
-              nzp >= 0 ? faces + ((size_t)nzp * 3 + 2) * 256 + tid : nullptr, epoch, gx, gy, gz, ok);
+              nzp >= 0 ? faces + ((size_t)nzp * 3 + 2) * 256 + tid : nullptr, epoch, limit, gx, gy, gz, ok);
     Zg[mghost(MT, u, v)] = gx;
     Zg[mghost(u, MT, v)] = gy;
     Zg[mghost(u, v, MT)] = gz;
+    zx = gx;
     if (!ok) atomicCAS(&ws->error, 0, slot + 1);
   }
   __syncthreads();
   {
-    const int cb = 15 * jj + 255 * kk, gb = mghost(0, jj, kk) - jj - kk;
+    const int gb = mghost(0, jj, kk) - o;
+    #pragma unroll
     for (int s = 3 * MT - 3; s >= 0; --s) {
-      if ((unsigned)(s - jj - kk) < (unsigned)MT) {
-        const int c = s + cb, g = s + gb;
-        const float zx = Zg[g + 1], zy = Zg[g + MGY], zz = Zg[g + MGZ];
-        Zg[g] = Tt[c] + Dd[c] * (WX[c] * zx + WY[c] * zy + WZ[c] * zz);
+      if ((unsigned)(s - o) < (unsigned)MT) {
+        const int g = s + gb, k = s & (MT - 1);
+        const float zy = Zg[g + MGY], zz = Zg[g + MGZ];
+        zx = ct[k] + cd[k] * (cx[k] * zx + cy[k] * zy + cz[k] * zz);
+        Zg[g] = zx;
       }
       __syncthreads();
     }

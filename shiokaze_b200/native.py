@@ -44,7 +44,10 @@ class Config(ctypes.Structure):
         ("gain", ctypes.c_double),
         ("warm_start", ctypes.c_int),
         ("index_tile", ctypes.c_int),
-        ("reserved", ctypes.c_int * 4),
+        ("spin_limit", ctypes.c_int),
+        ("fault_skip_publish", ctypes.c_int),
+        ("device_mem_limit_mb", ctypes.c_int),
+        ("csr_preconditioner", ctypes.c_int),
     ]
 
 
@@ -90,7 +93,8 @@ class Result(ctypes.Structure):
         ("fp64_reresid", ctypes.c_double), ("ms_assemble", ctypes.c_double), ("ms_solve", ctypes.c_double),
         ("ms_update", ctypes.c_double), ("ms_total", ctypes.c_double), ("ms_h2d", ctypes.c_double),
         ("ms_d2h", ctypes.c_double), ("kernel_launches", ctypes.c_longlong),
-        ("volume_rhs_correct", ctypes.c_double), ("reserved", ctypes.c_double * 6),
+        ("volume_rhs_correct", ctypes.c_double), ("ms_fractions", ctypes.c_double),
+        ("ms_labelling", ctypes.c_double), ("ms_build", ctypes.c_double), ("reserved", ctypes.c_double * 3),
     ]
 
     def as_dict(self):
@@ -106,6 +110,7 @@ EXPORTS = [
     "shkz_b200_learned_get_params", "shkz_b200_learned_apply", "shkz_b200_learned_dims",
     "shkz_b200_learned_tensor", "shkz_b200_learned_backward", "shkz_b200_learned_train",
     "shkz_b200_learned_save", "shkz_b200_learned_load", "shkz_b200_conv3d", "shkz_b200_conv3d_noalloc",
+    "shkz_b200_host_alloc", "shkz_b200_host_free",
     "shkz_b200_set_target_volume", "shkz_b200_get_volume_state", "shkz_b200_set_volume_state",
     "shkz_b200_warm_start_size", "shkz_b200_get_warm_start", "shkz_b200_set_warm_start",
     "shkz_b200_learned_flops", "shkz_b200_extend_velocity_host", "shkz_b200_extend_velocity_device",
@@ -170,6 +175,10 @@ def load(path: str = LIB_PATH):
     L.shkz_b200_learned_load.argtypes = [P, ctypes.c_char_p]
     L.shkz_b200_conv3d.argtypes = [ctypes.c_int] * 7 + [P, P, P, P, ctypes.c_int, P]
     L.shkz_b200_conv3d_noalloc.argtypes = [ctypes.c_int] * 7 + [P, P, P, P, ctypes.c_int, P, P]
+    L.shkz_b200_host_alloc.argtypes = [ctypes.c_size_t]
+    L.shkz_b200_host_alloc.restype = P
+    L.shkz_b200_host_free.argtypes = [P]
+    L.shkz_b200_host_free.restype = None
     _lib = L
     return L
 

@@ -37,9 +37,60 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <thread>
 #include <vector>
 //
 SHKZ_USING_NAMESPACE
+//
+// Dense staging array in page-locked host memory (shkz_b200_host_alloc), so
+// the library's host<->device copies run at full link speed; falls back to
+// ordinary heap memory if page-locked memory cannot be had. Grows only.
+template <class T> class staging_array {
+public:
+	staging_array() = default;
+	staging_array( const staging_array & ) = delete;
+	staging_array &operator=( const staging_array & ) = delete;
+	~staging_array() { release(); }
+	void assign( size_t n, T value ) {
+		resize(n);
+		// filled in slices by the host's threads (a 256^3 face grid is 67 MB)
+		const size_t nt = std::max(1u,std::min(32u,std::thread::hardware_concurrency()));
+		const size_t chunk = (n+nt-1)/nt;
+		std::vector<std::thread> workers;
+		for( size_t t=0; t<nt; ++t ) {
+			const size_t b = t*chunk, e = std::min(n,b+chunk);
+			if( b < e ) workers.emplace_back([=]() { std::fill(m_data+b,m_data+e,value); });
+		}
+		for( auto &w : workers ) w.join();
+	}
+	void resize( size_t n ) {
+		if( n > m_capacity ) {
+			release();
+			m_data = static_cast<T *>(shkz_b200_host_alloc(n*sizeof(T)));
+			m_pinned = m_data != nullptr;
+			if( ! m_data ) m_data = new T[n];
+			m_capacity = n;
+		}
+		m_size = n;
+	}
+	T *data() { return m_data; }
+	const T *data() const { return m_data; }
+	size_t size() const { return m_size; }
+	T &operator[]( size_t i ) { return m_data[i]; }
+	const T &operator[]( size_t i ) const { return m_data[i]; }
+private:
+	void release() {
+		if( m_data ) {
+			if( m_pinned ) shkz_b200_host_free(m_data);
+			else delete [] m_data;
+		}
+		m_data = nullptr;
+		m_capacity = m_size = 0;
+	}
+	T *m_data {nullptr};
+	size_t m_capacity {0}, m_size {0};
+	bool m_pinned {false};
+};
 //
 class macpressuresolver3_b200 : public macproject3_interface {
 protected:
@@ -59,15 +110,33 @@ protected:
 		m_solid_density = solid_density;
 	}
 	//
-	template <class T> static void pack( const array3<T> &a, std::vector<float> &v, std::vector<uint8_t> &m ) {
+	// Dense copy of what a(i,j,k) returns for every cell (as array3::linearize
+	// builds it: the background value, then the active values, then the fill
+	// value of inside cells that are not active) and the active bytes. Only
+	// tiles that hold active or filled cells are visited.
+	template <class T> static void pack( const array3<T> &a, staging_array<float> &v, staging_array<uint8_t> &m ) {
 		const shape3 s = a.shape();
-		v.resize(s.count());
-		m.resize(s.count());
-		a.const_parallel_all([&]( int i, int j, int k, const typename array3<T>::const_iterator &it ) {
+		v.assign(s.count(),(float)a.get_background_value());
+		m.assign(s.count(),0);
+		a.const_parallel_actives([&]( int i, int j, int k, const typename array3<T>::const_iterator &it ) {
 			const size_t n = i+(size_t)s.w*(j+(size_t)s.h*k);
 			v[n] = (float)it();
-			m[n] = it.active() ? 1 : 0;
+			m[n] = 1;
 		});
+		a.const_parallel_inside([&]( int i, int j, int k, const typename array3<T>::const_iterator &it ) {
+			if( ! it.active()) v[i+(size_t)s.w*(j+(size_t)s.h*k)] = (float)it();
+		});
+	}
+	// A face grid that reads zero everywhere (no active face, zero
+	// background, nothing filled) is passed as "no solid velocity".
+	static bool reads_zero( const array3<Real> &a ) {
+		if( a.get_background_value() != 0.0 || a.count()) return false;
+		bool filled (false);
+		a.interruptible_const_serial_inside([&](int i, int j, int k, const auto &it) {
+			filled = true;
+			return true;
+		});
+		return ! filled;
 	}
 	//
 	virtual void project( double dt,
@@ -102,9 +171,11 @@ protected:
 		pack(fluid,m_fluid,m_fluid_active);
 		const bool has_solid = levelset_exist_any(solid);
 		if( has_solid ) pack(solid,m_solid,m_solid_active);
+		bool svel_zero[3];
 		for( int dim=0; dim<3; ++dim ) {
 			pack(velocity[dim],m_vel[dim],m_vact[dim]);
-			pack(solid_velocity[dim],m_svel[dim],m_svact[dim]);
+			svel_zero[dim] = reads_zero(solid_velocity[dim]);
+			if( ! svel_zero[dim] ) pack(solid_velocity[dim],m_svel[dim],m_svact[dim]);
 			if( m_solid_density ) pack((*m_solid_density)[dim],m_dens[dim],m_dact[dim]);
 		}
 		console::dump( "Done. Took %s\n", timer.stock("pack_grids").c_str());
@@ -118,7 +189,7 @@ protected:
 		for( int dim=0; dim<3; ++dim ) {
 			a.velocity[dim] = m_vel[dim].data();
 			a.velocity_active[dim] = m_vact[dim].data();
-			a.solid_velocity[dim] = m_svel[dim].data();
+			a.solid_velocity[dim] = svel_zero[dim] ? nullptr : m_svel[dim].data();
 		}
 		m_p.resize(m_shape.count());
 		m_pact.resize(m_shape.count());
@@ -143,14 +214,27 @@ protected:
 			if( m_strict ) std::exit(1);
 			return;
 		}
+		// the reference's phase records (macpressuresolver3.cpp:95,168,218,232),
+		// from the library's device timings of the same phases
+		console::write(get_argument_name()+"_solid_fluid_fractions", res.ms_fractions);
+		console::write(get_argument_name()+"_labelling_cells", res.ms_labelling);
+		console::write(get_argument_name()+"_build_highres_linsystem", res.ms_build);
+		if( res.unknowns && m_param.gain && m_target_volume ) {
+			// the correction is added inside the system build's kernel: no time of its own
+			console::write(get_argument_name()+"_volume_correction", 0.0);
+		}
+		console::write(get_argument_name()+"_device_linsolve", res.ms_solve);
+		console::write(get_argument_name()+"_device_update_velocity", res.ms_update);
 		console::dump( "Done. Took %d iterations, Reresid=%e. Took %s\n", res.iterations, res.reresid, timer.stock("linsolve").c_str());
 		//
 		timer.tick(); console::dump( "Updating the velocity...");
+		// pressure and velocity back into the grids, tile by tile in parallel
+		// (parallel_all hands each thread whole tiles, so set() may allocate)
 		m_pressure.clear();
-		for( int k=0; k<m_shape.d; ++k ) for( int j=0; j<m_shape.h; ++j ) for( int i=0; i<m_shape.w; ++i ) {
+		m_pressure.parallel_all([&](int i, int j, int k, auto &it ) {
 			const size_t n = i+(size_t)m_shape.w*(j+(size_t)m_shape.h*k);
-			if( m_pact[n] ) m_pressure.set(i,j,k,m_p[n]);
-		}
+			if( m_pact[n] ) it.set(m_p[n]);
+		});
 		velocity.parallel_actives([&](int dim, int i, int j, int k, auto &it, int tn ) {
 			const shape3 fs = m_shape.face(dim);
 			const size_t n = i+(size_t)fs.w*(j+(size_t)fs.h*k);
@@ -277,8 +361,8 @@ protected:
 	std::vector<double> m_prev_host;
 	bool m_prev_pending {false};
 	// host staging
-	std::vector<float> m_fluid, m_solid, m_vel[3], m_svel[3], m_dens[3], m_p;
-	std::vector<uint8_t> m_fluid_active, m_solid_active, m_vact[3], m_svact[3], m_dact[3], m_pact;
+	staging_array<float> m_fluid, m_solid, m_vel[3], m_svel[3], m_dens[3], m_p;
+	staging_array<uint8_t> m_fluid_active, m_solid_active, m_vact[3], m_svact[3], m_dact[3], m_pact;
 };
 //
 extern "C" module * create_instance() {

@@ -24,6 +24,7 @@
 #include "shkz_b200.h"
 #include <algorithm>
 #include <cstring>
+#include <string>
 #include <utility>
 #include <vector>
 //
@@ -49,6 +50,9 @@ protected:
 		int device = m_cfg.device;
 		config.get_integer("B200.Device",device,"CUDA device ordinal");
 		m_cfg.device = device;
+		std::string pre (m_cfg.csr_preconditioner == SHKZ_B200_PRECOND_MIC0 ? "mic0" : "none");
+		config.get_string("B200.Preconditioner",pre,"none (as the shipped pcg runs) or mic0 (its MIC(0) applied)");
+		m_cfg.csr_preconditioner = pre == "mic0" ? SHKZ_B200_PRECOND_MIC0 : SHKZ_B200_PRECOND_NONE;
 	}
 	//
 	virtual Result solve( const RCMatrix_interface<size_t,double> *A, const RCMatrix_vector_interface<size_t,double> *b,

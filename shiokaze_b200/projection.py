@@ -101,6 +101,9 @@ class MacPressureSolver3:
         c.gain = float(g("Gain", c.gain))
         c.warm_start = int(bool(g("WarmStart", c.warm_start)))
         c.index_tile = int(g("TileSize", c.index_tile))
+        c.spin_limit = int(g("B200.SpinLimit", c.spin_limit))
+        c.fault_skip_publish = int(g("B200.FaultSkipPublish", c.fault_skip_publish))
+        c.device_mem_limit_mb = int(g("B200.DeviceMemoryLimitMB", c.device_mem_limit_mb))
         if self._ctx is not None:
             self._ctx.set_config(c)
 

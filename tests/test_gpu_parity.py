@@ -268,6 +268,72 @@ def test_solve_csr_matches_shipped_pcg(golden):
     assert rel_inf(p, g["pressure_shipped"]) <= max(PARITY_TOL, 10 * float(g["tol"]))
 
 
+def test_solve_csr_mic0_matches_reference_mic0(golden):
+    """shkz_b200_solve_csr with csr_preconditioner = MIC0 on the reference's own
+    assembled CSR: the generic-matrix MIC(0) (factor and level-scheduled sweeps
+    on the device) against the reference's MIC(0)-PCG on the same system:
+    iteration count within max(1, 2 %) and pressure within PARITY_TOL."""
+    import ctypes
+    from shiokaze_b200 import native
+    name, g = golden
+    sc = GoldenScene(g)
+    n = int(g["rhs"].size)
+    if n == 0:
+        return
+    cfg = native.default_config()
+    cfg.residual = float(g["tol"])
+    cfg.csr_preconditioner = native.PRECOND_MIC0
+    ctx = native.Context(cfg)
+    indptr = np.ascontiguousarray(g["indptr"], np.int64)
+    indices = np.ascontiguousarray(g["indices"], np.int64)
+    data = np.ascontiguousarray(g["data"], np.float64)
+    b = np.ascontiguousarray(g["rhs"], np.float64)
+    x = np.zeros(n, np.float64)
+    res = native.Result()
+    rc = native.load().shkz_b200_solve_csr(ctx.handle, n, indptr.ctypes.data, indices.ctypes.data, data.ctypes.data,
+                                           b.ctypes.data, x.ctypes.data, ctypes.byref(res))
+    assert rc == 0
+    it_ref = int(g["iterations_mic0"])
+    assert abs(res.iterations - it_ref) <= max(1, int(0.02 * it_ref)), (res.iterations, it_ref)
+    assert res.reresid <= float(g["tol"])
+    idx = oracle.assemble(sc, *oracle.fractions(sc)).index
+    mask = idx >= 0
+    p = np.zeros(idx.shape, np.float32)
+    p[mask] = x[idx[mask]].astype(np.float32)
+    assert rel_inf(p, g["pressure"]) <= PARITY_TOL
+
+
+def test_solve_csr_mic0_apply_matches_oracle(golden):
+    """One application of the CSR MIC(0) (a single PCG step from x0 = 0 with
+    tolerance 1 returns x = alpha z0): z0 against the oracle's MIC(0) apply,
+    which is bit-exact against the reference header's factor and sweeps."""
+    import ctypes
+    from shiokaze_b200 import native
+    name, g = golden
+    n = int(g["rhs"].size)
+    if n == 0:
+        return
+    indptr = np.ascontiguousarray(g["indptr"], np.int64)
+    indices = np.ascontiguousarray(g["indices"], np.int64)
+    data = np.ascontiguousarray(g["data"], np.float64)
+    b = np.ascontiguousarray(g["rhs"], np.float64)
+    S = oracle.System(index=None, n=n, indptr=indptr, indices=indices, data=data, rhs=b)
+    z, _ = oracle.mic0_apply(S, b)
+    cfg = native.default_config()
+    cfg.residual = 1e30  # stops after the first step
+    cfg.csr_preconditioner = native.PRECOND_MIC0
+    ctx = native.Context(cfg)
+    x = np.zeros(n, np.float64)
+    res = native.Result()
+    rc = native.load().shkz_b200_solve_csr(ctx.handle, n, indptr.ctypes.data, indices.ctypes.data, data.ctypes.data,
+                                           b.ctypes.data, x.ctypes.data, ctypes.byref(res))
+    assert rc == 0 and res.iterations == 1
+    # x = alpha z0 with alpha = (z0.b) / (z0.A z0)
+    Az = oracle.spmv(S, z)
+    alpha = float(z @ b) / float(z @ Az)
+    assert np.abs(x - alpha * z).max() <= 1e-12 * np.abs(alpha * z).max()
+
+
 def test_tile_activity_matches_reference(golden):
     """Tile activity: the pool holds exactly the 8^3 tiles in which the
     reference's pressure grid has an active cell (its allocated tiles)."""

@@ -116,6 +116,37 @@ def test_streamfunc_projection_runs_on_pcg_b200(n, seed, tol):
         assert rel_inf(got.velocity[d], ref.velocity[d]) <= tol_v, (d, rel_inf(got.velocity[d], ref.velocity[d]))
 
 
+@pytest.mark.skipif(not (ref_runner.ref_available("float") and os.path.exists(PCG_PLUGIN)),
+                    reason="needs the compiled reference harness and the pcg_b200 module")
+@pytest.mark.parametrize("projection", ["macpressuresolver3", "macstreamfuncsolver3"])
+def test_pcg_b200_mic0_matches_reference_mic0(projection):
+    """LinSolver=pcg_b200 with B200.Preconditioner=mic0 (the generic-matrix
+    MIC(0) on the device) against the reference's own PCG loop with its
+    header's MIC(0) applied (LinSolver=refmic0, RefMode=mic0), under both
+    projections that solve through the LinSolver plugin."""
+    sc = scenes.dambreak_sphere(n=24, seed=3, tol=1e-6)
+    extra = {"Projection": projection}
+    ref = ref_runner.run_reference(sc, linsolver="refmic0", mode="mic0", dump_system=False, extra=extra)
+    got = ref_runner.run_reference(sc, linsolver="pcg_b200", dump_system=False,
+                                   extra=dict(extra, **{"B200.Preconditioner": "mic0"}), extra_libpath=[PKG])
+    # each projection's own console line per solve: "Took N iterations" (then ", Reresid" or ". Reresid")
+    import re
+    its_ref = [int(c) for c in re.findall(r"Took (\d+) iterations", ref.stdout)]
+    its_got = [int(c) for c in re.findall(r"Took (\d+) iterations", got.stdout)]
+    assert len(its_got) == len(its_ref) > 0, (its_got, its_ref)
+    # The pressure system stops within 2 %. The stream-function system needs
+    # about twice the iterations and stops 3 % from the reference (303 against
+    # 313 at this scene); its bar is the 5 % that the dot products' summation
+    # order alone needs for unpreconditioned CG on the pressure system
+    # (test_pcg_b200_matches_reference_pcg).
+    spread = 0.02 if projection == "macpressuresolver3" else 0.05
+    for a, b in zip(its_got, its_ref):
+        assert abs(a - b) <= max(1, int(spread * b)), (its_got, its_ref)
+    for d in range(3):
+        np.testing.assert_array_equal(got.velocity_active[d], ref.velocity_active[d])
+        assert rel_inf(got.velocity[d], ref.velocity[d]) <= 1e-5, (d, rel_inf(got.velocity[d], ref.velocity[d]))
+
+
 FLIP_PLUGIN = os.path.join(PKG, "libshiokaze_macnbflip3_b200.so")
 
 
