@@ -43,22 +43,28 @@ pytestmark = pytest.mark.gpu
 
 PARITY_TOL = 1e-5
 
+# name: (scene, whether the pressure bar comes from the sensitivity fixture)
 CASES = {
-    "sloshing_tank_256": lambda s: s.sloshing_tank(n=256, seed=0, tol=1e-6),
-    "splash_384": lambda s: s.splash(n=384, seed=0, tol=1e-6),
+    "sloshing_tank_256": (lambda s: s.sloshing_tank(n=256, seed=0, tol=1e-6), False),
+    "splash_384": (lambda s: s.splash(n=384, seed=0, tol=1e-6), True),
 }
 
 
 def pressure_bars(name):
     """(bar on the pressure against the reference's, bar on the distance to the
-    FP64 tight solve or None)."""
+    FP64 tight solve or None). tests/golden/sensitivity_<name>.json holds the
+    reference's own algorithm on FP32-rounded inputs; at 256^3 (made by
+    ``python -m oracle.sensitivity --scene sloshing_tank --n 256``) those runs
+    move its pressure by up to 1.4e-5 and its count to 158-161, and the device
+    still meets PARITY_TOL there."""
     path = os.path.join(GOLDEN, f"sensitivity_{name}.json")
     if not os.path.exists(path):
         return PARITY_TOL, None
     runs = json.load(open(path))["runs"]
     moved = max(r["pressure_vs_reference"] for r in runs.values())
     farthest = max(r["pressure_vs_tight"] for r in runs.values())
-    return max(PARITY_TOL, 2.0 * moved), 1.25 * farthest
+    p_bar = max(PARITY_TOL, 2.0 * moved) if CASES[name][1] else PARITY_TOL
+    return p_bar, 1.25 * farthest
 
 
 def rel_inf(a, b):
@@ -73,7 +79,7 @@ def test_full_size_matches_compiled_reference(name):
     from shiokaze_b200.projection import MacPressureSolver3, grids_from_scene
     if not ref_runner.ref_available("float"):
         pytest.skip("compiled reference (oracle/_ref) not built")
-    sc = CASES[name](scenes)
+    sc = CASES[name][0](scenes)
     s = MacPressureSolver3({"Residual": sc.tol, "B200.FP64Reference": True})
     s.initialize((sc.nx, sc.ny, sc.nz), sc.dx)
     vel, solid, svel, fluid = grids_from_scene(sc)
