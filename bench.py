@@ -59,6 +59,11 @@ ALGO_BYTES = {
 # One fused MIC(0)-PCG iteration: stencil pass 32 + sweep pair 72.
 ITER_BYTES = 104
 
+# library kernels one splat call launches: bin, tile scan, three scan passes,
+# scatter, sort, three face compactions, three work counts, work scan, three
+# face sorts, three gathers, clear
+SPLAT_LAUNCHES = 21
+
 # FLIP splat workload (--workload flip_splat): the splat and combined grid
 # velocity before a projection, on the 256^3 sloshing tank with particles in
 # the 3-cell narrow band at 8 per cell. Algorithmic bytes: every particle's
@@ -368,7 +373,7 @@ def run_splat(args):
                            "l2": "particle records 0.2 GB + face grids 0.25 GB > 126 MB L2 (no flush needed)",
                            "step": "device velocity restore + one splat"},
                 "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(),
-                "gpu_launches": args.steps * 19}
+                "gpu_launches": args.steps * SPLAT_LAUNCHES}
         print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:

@@ -52,6 +52,7 @@ struct shkz_b200_ctx {
       *sched = nullptr, *bsum = nullptr, *total = nullptr;
   // pool arrays
   float *diag = nullptr, *offx = nullptr, *offy = nullptr, *offz = nullptr, *d32 = nullptr;
+  float *upx = nullptr, *upy = nullptr, *upz = nullptr;  // upper weights of the backward sweep
   double *diag64 = nullptr, *offx64 = nullptr, *offy64 = nullptr, *offz64 = nullptr, *rhs64 = nullptr,
          *colsum = nullptr, *dmic64 = nullptr, *x64 = nullptr, *r64 = nullptr, *xref64 = nullptr,
          *p64 = nullptr, *q64 = nullptr, *z64 = nullptr;
@@ -103,8 +104,10 @@ struct shkz_b200_ctx {
   long long cap_sp_particles = 0;
   int *sp_faces = nullptr, *sp_sorted = nullptr, *sp_face_bin = nullptr, *sp_nfaces = nullptr, *sp_work = nullptr;
   long long cap_sp_list = 0;
-  int *sp_start = nullptr, *sp_tiles = nullptr;
-  long long cap_sp_buckets = 0;
+  int *sp_count = nullptr, *sp_tile_start = nullptr, *sp_tiles = nullptr;
+  uint8_t *sp_tile_act = nullptr;
+  long long cap_sp_tiles = 0;
+  bool sp_dirty = false;  // bucket counters may be nonzero: a call stopped before clearing them
   uint8_t *sp_act[3] = {};
   size_t cap_sp_faces[3] = {0, 0, 0};
   float *sp_mass[3] = {}, *sp_mom[3] = {};  // optional outputs (host path)
@@ -288,6 +291,7 @@ static int ensure_pool(shkz_b200_ctx *ctx, int K) {
   GROW(colsum, n); GROW(dmic64, n); GROW(x64, n); GROW(r64, n); GROW(xref64, n);
   GROW(p64, n); GROW(q64, n); GROW(z64, n);
   GROW(x, n); GROW(r, n); GROW(p, n); GROW(q, n); GROW(z, n); GROW(t, n); GROW(p32, n); GROW(pb, n);
+  GROW(upx, n); GROW(upy, n); GROW(upz, n);
   GROW(partials, (size_t)2 * cap + 4 * 8192);
   GROW(wflags, (size_t)cap);
   GROW(faces_f, (size_t)cap * 3 * 64);
@@ -403,7 +407,7 @@ extern "C" void shkz_b200_destroy(shkz_b200_ctx *ctx) {
                   ctx->h_vact[0], ctx->h_vact[1], ctx->h_vact[2], ctx->h_pact, ctx->flags, ctx->unk, ctx->tile_count,
                   ctx->tile_state, ctx->pool_tile, ctx->nbr, ctx->level_count, ctx->sched, ctx->bsum, ctx->total,
                   ctx->diag, ctx->offx, ctx->offy, ctx->offz, ctx->d32, ctx->diag64, ctx->offx64, ctx->offy64,
-                  ctx->offz64, ctx->rhs64, ctx->colsum, ctx->dmic64, ctx->x64, ctx->r64, ctx->xref64, ctx->p64, ctx->q64,
+                  ctx->offz64, ctx->rhs64, ctx->upx, ctx->upy, ctx->upz, ctx->colsum, ctx->dmic64, ctx->x64, ctx->r64, ctx->xref64, ctx->p64, ctx->q64,
                   ctx->z64, ctx->x, ctx->r,
                   ctx->p, ctx->q, ctx->z, ctx->t, ctx->p32, ctx->partials, ctx->out4, ctx->counter, ctx->st,
                   ctx->wflags, ctx->faces_f, ctx->faces_b, ctx->ws, ctx->st_scratch, ctx->mcount, ctx->mstate,
@@ -413,7 +417,7 @@ extern "C" void shkz_b200_destroy(shkz_b200_ctx *ctx) {
                   ctx->ext_a[0], ctx->ext_a[1], ctx->ext_a[2], ctx->ext_flag, ctx->sp_raw, ctx->sp_posm,
                   ctx->sp_vc[0], ctx->sp_vc[1], ctx->sp_vc[2], ctx->sp_key, ctx->sp_rank, ctx->sp_list, ctx->sp_sposm,
                   ctx->sp_svc, ctx->sp_faces, ctx->sp_sorted, ctx->sp_face_bin, ctx->sp_nfaces, ctx->sp_work,
-                  ctx->sp_start, ctx->sp_tiles, ctx->sp_act[0], ctx->sp_act[1], ctx->sp_act[2], ctx->sp_mass[0],
+                  ctx->sp_count, ctx->sp_tile_start, ctx->sp_tile_act, ctx->sp_tiles, ctx->sp_act[0], ctx->sp_act[1], ctx->sp_act[2], ctx->sp_mass[0],
                   ctx->sp_mass[1], ctx->sp_mass[2], ctx->sp_mom[0], ctx->sp_mom[1], ctx->sp_mom[2],
                   ctx->sp_sact[0], ctx->sp_sact[1], ctx->sp_sact[2]};
   for (void *p : ptrs)
@@ -452,6 +456,9 @@ static PoolSystem pool_system(shkz_b200_ctx *ctx) {
   S.offx64 = ctx->offx64;
   S.offy64 = ctx->offy64;
   S.offz64 = ctx->offz64;
+  S.upx = ctx->upx;
+  S.upy = ctx->upy;
+  S.upz = ctx->upz;
   return S;
 }
 
@@ -828,6 +835,7 @@ static int project_device(shkz_b200_ctx *ctx, const shkz_b200_project_args *a, s
   CoeffOutputs co{ctx->diag, ctx->offx, ctx->offy, ctx->offz, ctx->diag64, ctx->offx64, ctx->offy64, ctx->offz64,
                   ctx->rhs64};
   launch_coeff(in, ctx->flags, ctx->pool_tile, K, ctx->unk, co, s);
+  if (K > 0) launch_upper_weights(pool_system(ctx), ctx->upx, ctx->upy, ctx->upz, s);
   cudaEventRecord(ctx->ev[10], s);
   const bool warm = K > 0 && ctx->cfg.warm_start;
   if (warm) {
@@ -1111,11 +1119,12 @@ extern "C" int shkz_b200_extend_velocity_host(shkz_b200_ctx *ctx, const shkz_b20
 // FLIP splat before the projection (macflipliquid3.cpp:135-151): kernels in
 // splat.cu.
 
-static long long splat_buckets(int nx, int ny, int nz, long long base[3]) {
+// 8x8x8 tiles of the three axes' edge grids, numbered one axis after another
+static long long splat_tiles(int nx, int ny, int nz, long long base[3]) {
   long long total = 0;
   for (int d = 0; d < 3; ++d) {
     base[d] = total;
-    total += (long long)(nx + (d != 0)) * (ny + (d != 1)) * (nz + (d != 2));
+    total += (long long)((nx + (d != 0) + 7) / 8) * ((ny + (d != 1) + 7) / 8) * ((nz + (d != 2) + 7) / 8);
   }
   return total;
 }
@@ -1124,8 +1133,8 @@ static int validate_splat(const shkz_b200_splat_args *a) {
   if (!a || a->nx < 1 || a->ny < 1 || a->nz < 1 || !(a->dx > 0.0) || a->count < 0) return SHKZ_B200_ERR_ARG;
   if (a->nx > 65536 || a->ny > 65536 || a->nz > 65536) return SHKZ_B200_ERR_LIMIT;
   long long base[3];
-  const long long buckets = splat_buckets(a->nx, a->ny, a->nz, base);
-  if (buckets + 1 >= ((long long)1 << 31) || 3 * a->count >= ((long long)1 << 31)) return SHKZ_B200_ERR_LIMIT;
+  const long long tiles = splat_tiles(a->nx, a->ny, a->nz, base);
+  if (512 * tiles >= ((long long)1 << 31) || 3 * a->count >= ((long long)1 << 31)) return SHKZ_B200_ERR_LIMIT;
   // the velocity (in/out) and the splat grid (out) are each all three axes or
   // none, and at least one of them is given
   const bool vel0 = a->velocity[0] != nullptr;
@@ -1152,7 +1161,7 @@ static int splat_device(shkz_b200_ctx *ctx, const shkz_b200_splat_args *a, const
                         const SplatGrid &grid) {
   cudaStream_t s = ctx->stream;
   SplatBuffers B{};
-  B.buckets = splat_buckets(a->nx, a->ny, a->nz, B.bucket_base);
+  B.tiles = splat_tiles(a->nx, a->ny, a->nz, B.tile_base);
   B.apic = a->offset_apic >= 0;
   const long long n = a->count;
   if (n > ctx->cap_sp_particles) {
@@ -1167,10 +1176,19 @@ static int splat_device(shkz_b200_ctx *ctx, const shkz_b200_splat_args *a, const
   }
   if (!ctx->sp_nfaces) GROW(sp_nfaces, 4);
   if (!ctx->sp_work) GROW(sp_work, 3 * kSplatWorkBins);
-  if (B.buckets + 1 > ctx->cap_sp_buckets) {
-    GROW(sp_start, B.buckets + 1);
-    GROW(sp_tiles, scan_tile_count(B.buckets + 1));
-    ctx->cap_sp_buckets = B.buckets + 1;
+  if (B.tiles > ctx->cap_sp_tiles) {
+    GROW(sp_count, 512 * B.tiles);
+    GROW(sp_tile_act, B.tiles);
+    GROW(sp_tile_start, B.tiles + 1);
+    GROW(sp_tiles, scan_tile_count(B.tiles + 1));
+    ctx->cap_sp_tiles = B.tiles;
+    ctx->sp_dirty = true;
+  }
+  // counters and tile flags are zero between calls; set them once when new
+  // or after a call that stopped before its clear pass
+  if (ctx->sp_dirty) {
+    SHKZ_CUDA_TRY(cudaMemsetAsync(ctx->sp_count, 0, (size_t)ctx->cap_sp_tiles * 512 * sizeof(int), s));
+    SHKZ_CUDA_TRY(cudaMemsetAsync(ctx->sp_tile_act, 0, (size_t)ctx->cap_sp_tiles, s));
   }
   // a particle activates at most 8 faces per axis
   size_t nf[3];
@@ -1198,7 +1216,9 @@ static int splat_device(shkz_b200_ctx *ctx, const shkz_b200_splat_args *a, const
   B.posm = ctx->sp_posm;
   B.key = ctx->sp_key;
   B.rank = ctx->sp_rank;
-  B.start = ctx->sp_start;
+  B.count = ctx->sp_count;
+  B.tile_act = ctx->sp_tile_act;
+  B.tile_start = ctx->sp_tile_start;
   B.list = ctx->sp_list;
   B.sposm = ctx->sp_sposm;
   B.svc = ctx->sp_svc;
@@ -1207,19 +1227,21 @@ static int splat_device(shkz_b200_ctx *ctx, const shkz_b200_splat_args *a, const
   B.face_bin = ctx->sp_face_bin;
   B.work = ctx->sp_work;
   B.nfaces = ctx->sp_nfaces;
-  SHKZ_CUDA_TRY(cudaMemsetAsync(ctx->sp_start, 0, (size_t)(B.buckets + 1) * sizeof(int), s));
   SHKZ_CUDA_TRY(cudaMemsetAsync(ctx->sp_nfaces, 0, 4 * sizeof(int), s));
   SHKZ_CUDA_TRY(cudaMemsetAsync(ctx->sp_work, 0, 3 * kSplatWorkBins * sizeof(int), s));
   SplatRecords R{static_cast<const unsigned char *>(particles), n, a->stride, a->offset_position,
                  a->offset_velocity, a->offset_mass, a->offset_apic, a->offset_bullet, a->splat_bullet != 0};
+  ctx->sp_dirty = true;
   launch_splat_bin(R, a->nx, a->ny, a->nz, a->dx, B, s);
-  launch_exclusive_scan(ctx->sp_start, B.buckets + 1, ctx->sp_tiles, s);
+  launch_splat_bucket_scan(B, ctx->sp_tiles, s);
   launch_splat_scatter(n, B, s);
   launch_splat_gather(a->nx, a->ny, a->nz, a->dx, B, grid, s);
+  launch_splat_clear(B, s);
   SHKZ_CUDA_TRY(cudaGetLastError());
   int over = 0;
   SHKZ_CUDA_TRY(cudaMemcpyAsync(&over, ctx->sp_nfaces + 3, sizeof(int), cudaMemcpyDeviceToHost, s));
   SHKZ_CUDA_TRY(cudaStreamSynchronize(s));
+  ctx->sp_dirty = false;
   return over ? SHKZ_B200_ERR_LIMIT : 0;
 }
 

@@ -31,6 +31,9 @@ struct PoolSystem {
   const int *nbr;        // [K][6] pool index of neighbour tiles or -1
   const int *sched;      // [K] pool indices ordered by wavefront level
   const float *diag, *offx, *offy, *offz;
+  // upper weights: the lower weight of the +x/+y/+z neighbour cell (across
+  // the tile face where needed), for the backward MIC(0) sweep
+  const float *upx, *upy, *upz;
   const double *diag64, *offx64, *offy64, *offz64;
   // 16^3 macro tiles (2x2x2 pool tiles) for the MIC(0) sweeps
   int KM;
@@ -75,9 +78,16 @@ struct SplatRecords {
 struct SplatBuffers {
   float4 *posm;            // per particle: p, mass
   float4 *vc[3];           // per particle and axis d: u_d, c[d]
-  int *key, *rank;         // [3][count]: global edge bucket (-1: does not splat), slot in it
-  int *start;              // buckets + 1 counters, scanned into bucket starts
-  int *list;               // [3 count] particle indices, bucket by bucket, arrival order inside one
+  int *key, *rank;         // [3][count]: edge bucket slot (-1: does not splat), arrival rank in it
+  // Edge buckets live in 8x8x8 tiles of each axis' edge grid, 512 slots a
+  // tile (splat.cu: bucket_slot). count holds a bucket's particles, then its
+  // offset inside the tile's run; tile_start the first list position of each
+  // tile. count and tile_act are zero between calls: a call touches and then
+  // clears only the tiles its particles reach.
+  int *count;              // [tiles * 512]
+  uint8_t *tile_act;       // [tiles] the tile holds a particle
+  int *tile_start;         // [tiles + 1], exclusive scan of the tiles' particle counts
+  int *list;               // [3 count] d * count + particle index, bucket by bucket, arrival order inside one
   float4 *sposm, *svc;     // [3 count] posm and vc[d] bucket by bucket, index order inside one
   uint8_t *act[3];         // faces activated by the splat
   int *faces;              // active faces of each axis, listed from face_off[d]
@@ -86,8 +96,8 @@ struct SplatBuffers {
   int *work;               // [3][kSplatWorkBins] work-class counts, then cursors
   int *nfaces;             // [4]: list lengths of the three axes, then a bucket over kSplatBucketLimit (flag)
   long long face_off[3];
-  long long bucket_base[3];
-  long long buckets;
+  long long tile_base[3];  // first tile of each axis
+  long long tiles;
   int apic;
 };
 struct SplatGrid {
@@ -100,8 +110,13 @@ void launch_splat_bin(const SplatRecords &R, int nx, int ny, int nz, double dx, 
                       cudaStream_t s);
 size_t scan_tile_count(long long n);
 void launch_exclusive_scan(int *data, long long n, int *tile_sums, cudaStream_t s);
+// each reached tile's bucket counts into offsets inside it, then the tiles'
+// starts (tile_sums: scratch of scan_tile_count(tiles + 1) ints)
+void launch_splat_bucket_scan(const SplatBuffers &B, int *tile_sums, cudaStream_t s);
 // bucket lists, then the particles' data copied into bucket order
 void launch_splat_scatter(long long count, const SplatBuffers &B, cudaStream_t s);
+// counts and tile flags of the reached tiles back to zero
+void launch_splat_clear(const SplatBuffers &B, cudaStream_t s);
 // active-face lists ordered by work, then the per-face sums and the combined velocity
 void launch_splat_gather(int nx, int ny, int nz, double dx, const SplatBuffers &B, const SplatGrid &G,
                          cudaStream_t s);

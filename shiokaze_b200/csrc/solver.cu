@@ -1078,61 +1078,11 @@ __global__ void __launch_bounds__(256, 2) k_mic_backward16(PoolSystem S, const f
   const int tid = threadIdx.x, jj = tid & 15, kk = tid >> 4;
   if (tid < 8) sub[tid] = S.msub[mt * 8 + tid];
   __syncthreads();
-  macro_load5(sub, t, d32, S.offx, S.offy, S.offz, Tt, Dd, WX, WY, WZ);
+  // the upper weights come precomputed (launch_upper_weights): W?[c] is the
+  // lower weight of the +x/+y/+z neighbour cell, across the macro face where
+  // needed, so the sweep reads them at the cell's own index
+  macro_load5(sub, t, d32, S.upx, S.upy, S.upz, Tt, Dd, WX, WY, WZ);
   const int nxp = S.mnbr[mt * 6 + NB_XP], nyp = S.mnbr[mt * 6 + NB_YP], nzp = S.mnbr[mt * 6 + NB_ZP];
-  float wxv = 0.f, wyv = 0.f, wzv = 0.f;
-  {
-    // upper weights across the macro faces: lower weights of the +x/+y/+z
-    // macro neighbours' first column/row/plane, from their pool sub-tiles
-    const int u = tid & 15, v = tid >> 4;
-    if (nxp >= 0) {  // cell (0, u, v) of the +x macro tile
-      const int pt = S.msub[nxp * 8 + 0 + 2 * (u >> 3) + 4 * (v >> 3)];
-      if (pt >= 0) wxv = S.offx[(size_t)pt * SHKZ_TC + 8 * (u & 7) + 64 * (v & 7)];
-    }
-    if (nyp >= 0) {  // cell (u, 0, v) of the +y macro tile
-      const int pt = S.msub[nyp * 8 + (u >> 3) + 4 * (v >> 3)];
-      if (pt >= 0) wyv = S.offy[(size_t)pt * SHKZ_TC + (u & 7) + 64 * (v & 7)];
-    }
-    if (nzp >= 0) {  // cell (u, v, 0) of the +z macro tile
-      const int pt = S.msub[nzp * 8 + (u >> 3) + 2 * (v >> 3)];
-      if (pt >= 0) wzv = S.offz[(size_t)pt * SHKZ_TC + (u & 7) + 8 * (v & 7)];
-    }
-  }
-  __syncthreads();
-  {
-    // upper weights in place: W?[c] <- the lower weight of the +x/+y/+z
-    // neighbour cell (the macro neighbour's, across the face), so the sweep
-    // reads them at the cell's own index. Thread (jj, kk) owns its x-row; the
-    // y/z shifts read other threads' rows, so all reads precede all writes.
-    const int r0 = MT * jj + MT * MT * kk;
-    float ux[MT], uy[MT], uz[MT];
-    #pragma unroll
-    for (int i = 0; i < MT; ++i) {
-      ux[i] = i < MT - 1 ? WX[r0 + i + 1] : 0.f;
-      uy[i] = jj < MT - 1 ? WY[r0 + i + MT] : 0.f;
-      uz[i] = kk < MT - 1 ? WZ[r0 + i + MT * MT] : 0.f;
-    }
-    __syncthreads();
-    // the +x face weight of row (jj, kk) is entry jj + 16 kk of the +x
-    // neighbour's column, held by thread jj + 16 kk (this thread); the +y
-    // face weight of cell (i, 15, kk) and the +z weight of cell (i, jj, 15)
-    // are entries i + 16 kk and i + 16 jj, gathered through shared memory
-    #pragma unroll
-    for (int i = 0; i < MT; ++i) {
-      WX[r0 + i] = ux[i];
-      WY[r0 + i] = uy[i];
-      WZ[r0 + i] = uz[i];
-    }
-    WX[r0 + MT - 1] = wxv;
-    __syncthreads();
-    {
-      // tid = u + 16 v holds the +y weight of cell (u, 15, v) and the +z
-      // weight of cell (u, v, 15)
-      const int u = tid & 15, v = tid >> 4;
-      WY[u + MT * (MT - 1) + MT * MT * v] = wyv;
-      WZ[u + MT * v + MT * MT * (MT - 1)] = wzv;
-    }
-  }
   __syncthreads();
   // the thread's x-row in registers, rotated as in the forward sweep: slot k
   // holds cell (k - o) mod 16
@@ -1207,6 +1157,38 @@ __global__ void __launch_bounds__(256, 2) k_mic_backward16(PoolSystem S, const f
     }
   }
   sweep_end(ws, epoch);
+}
+
+// Upper weights of every pool cell: the lower weight of the +x/+y/+z
+// neighbour cell (A(i, i+e) = -off?(i+e)), from the neighbour tile across a
+// tile face, zero where that tile is not in the pool. They depend on the
+// matrix only, so the backward MIC(0) sweep stages them instead of shifting
+// the lower weights every iteration.
+__global__ void __launch_bounds__(256) k_upper_weights(PoolSystem S, float *__restrict__ upx,
+                                                       float *__restrict__ upy, float *__restrict__ upz) {
+  const long long n = (long long)S.K * SHKZ_TC;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int pt = (int)(i >> 9), c = (int)(i & 511);
+    const int ii = c & 7, jj = (c >> 3) & 7, kk = c >> 6;
+    const size_t base = (size_t)pt * SHKZ_TC;
+    float ux = 0.f, uy = 0.f, uz = 0.f;
+    if (ii < 7) ux = S.offx[base + c + 1];
+    else if (S.nbr[pt * 6 + NB_XP] >= 0) ux = S.offx[(size_t)S.nbr[pt * 6 + NB_XP] * SHKZ_TC + c - 7];
+    if (jj < 7) uy = S.offy[base + c + 8];
+    else if (S.nbr[pt * 6 + NB_YP] >= 0) uy = S.offy[(size_t)S.nbr[pt * 6 + NB_YP] * SHKZ_TC + c - 56];
+    if (kk < 7) uz = S.offz[base + c + 64];
+    else if (S.nbr[pt * 6 + NB_ZP] >= 0) uz = S.offz[(size_t)S.nbr[pt * 6 + NB_ZP] * SHKZ_TC + c - 448];
+    upx[i] = ux;
+    upy[i] = uy;
+    upz[i] = uz;
+  }
+}
+
+static int grid_for(long long n, int per, int cap);
+void launch_upper_weights(const PoolSystem &S, float *upx, float *upy, float *upz, cudaStream_t s) {
+  if (S.K <= 0) return;
+  count_launches(1);
+  k_upper_weights<<<grid_for((long long)S.K * SHKZ_TC, 256 * 4, 148 * 8), 256, 0, s>>>(S, upx, upy, upz);
 }
 
 size_t mic16_smem_forward() { return sizeof(float) * (MGC + 5 * MTC); }

@@ -64,6 +64,8 @@ void build_macro(const Geometry &G, const Geometry &M, const int *tile_count, co
                  const int *bsum, cudaStream_t s);
 void launch_fpcg_dots(int n, const float *z, const float *r, const float *q, double *partials, unsigned *counter,
                       SolverState *st, int init, cudaStream_t s);
+// upx/upy/upz of every pool cell from the lower weights and the tile neighbours
+void launch_upper_weights(const PoolSystem &S, float *upx, float *upy, float *upz, cudaStream_t s);
 void launch_rand_unknowns(int n, const float *diag, unsigned seed, float *e, cudaStream_t s);
 void launch_scale_f32(int n, float *a, float sc, cudaStream_t s);
 void launch_axpby_f32(int n, float a, const float *x, float b, float *y, cudaStream_t s);

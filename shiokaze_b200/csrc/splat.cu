@@ -15,7 +15,8 @@
 //            (u_d, c_d) into float4s, finds its edge bucket per axis and
 //            takes a slot in it with an atomic counter, and marks the 8 faces
 //            per axis it activates;
-//   scan     exclusive scan of the bucket counters into bucket starts;
+//   scan     in each tile of buckets a particle reached, the counters into
+//            offsets inside the tile; then the tiles' starts;
 //   scatter  every particle index into its bucket's slot;
 //   sort     one thread per slot: the slot's particle goes to the rank its
 //            index has in the bucket (the atomic slots are in arrival order)
@@ -28,11 +29,14 @@
 //            each twice: the query's loops run over all three axes but the
 //            bucket does not move along the face's own axis), sums
 //            tent-weighted mass and momentum (APIC term included), and
-//            combines with the grid velocity in place.
+//            combines with the grid velocity in place;
+//   clear    the reached tiles' counters back to zero.
 // Faces are dense, x fastest; axis d has (nx+(d==0)) x (ny+(d==1)) x
 // (nz+(d==2)) entries. Edge buckets of axis d cover (nx+(d!=0)) x
-// (ny+(d!=1)) x (nz+(d!=2)) edges; the three axes' buckets are numbered one
-// after another in a single counter array.
+// (ny+(d!=1)) x (nz+(d!=2)) edges, grouped in 8x8x8 tiles (bucket_slot); the
+// three axes' tiles are numbered one after another. Only tiles that hold a
+// particle are scanned and cleared, so the bucket bookkeeping costs in
+// proportion to the particles' band, not to the grid.
 #include <cmath>
 
 #include "common.cuh"
@@ -78,6 +82,25 @@ __device__ __forceinline__ double tent(float r, const DxDiv &X) {
   return 0.0 < v ? v : 0.0;
 }
 
+// Slot of the edge bucket e (edge coordinates on axis d, extents E): the
+// edge's 8x8x8 tile, numbered x fastest after the earlier axes' tiles, times
+// 512, plus the edge's place in the tile (x fastest).
+__device__ __forceinline__ int bucket_slot(const SplatBuffers &B, int d, const int E[3], const int e[3]) {
+  const long long T0 = (E[0] + 7) >> 3, T1 = (E[1] + 7) >> 3;
+  const long long tile = B.tile_base[d] + (e[0] >> 3) + T0 * ((e[1] >> 3) + T1 * (e[2] >> 3));
+  return (int)((tile << 9) | (e[0] & 7) | ((e[1] & 7) << 3) | ((e[2] & 7) << 6));
+}
+
+// [first, end) of a bucket's particles in the bucket-ordered list. In a tile
+// no particle reached every count is zero, so the range is empty.
+__device__ __forceinline__ int2 bucket_range(const SplatBuffers &B, int slot) {
+  const int t = slot >> 9;
+  const int t0 = __ldg(B.tile_start + t);
+  const int first = t0 + __ldg(B.count + slot);
+  const int end = (slot & 511) == 511 ? __ldg(B.tile_start + t + 1) : t0 + __ldg(B.count + slot + 1);
+  return make_int2(first, end);
+}
+
 __global__ void k_splat_bin(SplatRecords R, int nx, int ny, int nz, DxDiv X, SplatBuffers B) {
   const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= R.count) return;
@@ -106,9 +129,11 @@ __global__ void k_splat_bin(SplatRecords R, int nx, int ny, int nz, DxDiv X, Spl
       E[c] = n3[c] + (c != d);
       e[c] = edge_axis(p[c], X, c != d, E[c]);
     }
-    const int key = (int)(B.bucket_base[d] + e[0] + (long long)E[0] * (e[1] + (long long)E[1] * e[2]));
+    const int key = bucket_slot(B, d, E, e);
     B.key[slot] = key;
-    B.rank[slot] = atomicAdd(&B.start[key], 1);
+    const int rank = atomicAdd(&B.count[key], 1);
+    B.rank[slot] = rank;
+    if (rank == 0) B.tile_act[key >> 9] = 1;
     // faces this particle activates (macnbflip3.cpp:109-120): the cell below
     // the face-centred position and its +1 neighbours, clamped to the cells
     int pi[3];
@@ -233,6 +258,65 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_add(int *data, long long 
   store8(data, base, n, v);
 }
 
+// One warp per tile of 512 bucket counters. A tile that a particle reached
+// turns its counters into offsets inside the tile and writes its particle
+// total; every other tile's total is zero without reading its counters. The
+// entry after the last tile is zero as well, so that the exclusive scan of the
+// totals leaves the particle total there.
+constexpr int kTileWarps = 8;
+
+__global__ void __launch_bounds__(32 * kTileWarps) k_splat_tile_scan(SplatBuffers B) {
+  const long long t = (long long)blockIdx.x * kTileWarps + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (t > B.tiles) return;
+  if (t == B.tiles || !B.tile_act[t]) {
+    if (lane == 0) B.tile_start[t] = 0;
+    return;
+  }
+  // 16 counters a lane: the buffer is 16-byte aligned and a tile is 2 KB
+  int4 *c = reinterpret_cast<int4 *>(B.count + (t << 9) + lane * 16);
+  int v[16];
+  #pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int4 a = c[q];
+    v[4 * q] = a.x;
+    v[4 * q + 1] = a.y;
+    v[4 * q + 2] = a.z;
+    v[4 * q + 3] = a.w;
+  }
+  int sum = 0;
+  #pragma unroll
+  for (int q = 0; q < 16; ++q) sum += v[q];
+  int x = sum;
+  #pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  int run = x - sum;
+  #pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    const int k = v[q];
+    v[q] = run;
+    run += k;
+  }
+  #pragma unroll
+  for (int q = 0; q < 4; ++q) c[q] = make_int4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+  if (lane == 31) B.tile_start[t] = x;
+}
+
+// the reached tiles' counters and flags back to zero for the next call
+__global__ void __launch_bounds__(32 * kTileWarps) k_splat_tile_clear(SplatBuffers B) {
+  const long long t = (long long)blockIdx.x * kTileWarps + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (t >= B.tiles || !B.tile_act[t]) return;
+  int4 *c = reinterpret_cast<int4 *>(B.count + (t << 9) + lane * 16);
+  #pragma unroll
+  for (int q = 0; q < 4; ++q) c[q] = make_int4(0, 0, 0, 0);
+  __syncwarp();
+  if (lane == 0) B.tile_act[t] = 0;
+}
+
 __global__ void k_splat_scatter(long long count, SplatBuffers B) {
   const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= count) return;
@@ -240,7 +324,7 @@ __global__ void k_splat_scatter(long long count, SplatBuffers B) {
   for (int d = 0; d < 3; ++d) {
     const size_t slot = (size_t)d * count + n;
     const int key = B.key[slot];
-    if (key >= 0) B.list[B.start[key] + B.rank[slot]] = (int)n;
+    if (key >= 0) B.list[bucket_range(B, key).x + B.rank[slot]] = (int)slot;
   }
 }
 
@@ -250,19 +334,21 @@ __global__ void k_splat_scatter(long long count, SplatBuffers B) {
 // bucket contiguously and in the reference's order.
 __global__ void k_splat_sort_copy(long long count, SplatBuffers B) {
   const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int total = B.start[B.buckets];
+  const int total = B.tile_start[B.tiles];
   if (s >= total) return;
-  const int d = s < B.start[B.bucket_base[1]] ? 0 : (s < B.start[B.bucket_base[2]] ? 1 : 2);
-  const int n = B.list[s];
-  const int key = B.key[(size_t)d * count + n];
-  const int s0 = B.start[key], s1 = B.start[key + 1];
+  const int sl = B.list[s];  // d * count + particle
+  const int d = (int)(sl / count);
+  const long long n = sl - d * count;
+  const int2 range = bucket_range(B, B.key[sl]);
+  const int s0 = range.x, s1 = range.y;
   if (s1 - s0 > kSplatBucketLimit) {
     // refused (the call returns SHKZ_B200_ERR_LIMIT and the gather writes nothing)
     if (s == s0) B.nfaces[3] = 1;
     return;
   }
+  // one bucket holds one axis' entries, so d * count + particle orders them by particle
   int r = 0;
-  for (int t = s0; t < s1; ++t) r += B.list[t] < n;
+  for (int t = s0; t < s1; ++t) r += B.list[t] < sl;
   B.sposm[s0 + r] = B.posm[n];
   B.svc[s0 + r] = B.vc[d][n];
 }
@@ -326,8 +412,8 @@ __device__ __forceinline__ int face_visits(size_t f, int nx, int ny, int nz, con
     int q[3];
     bucket_coords<D>(k, fi, q);
     if (q[0] < 0 || q[0] >= E[0] || q[1] < 0 || q[1] >= E[1] || q[2] < 0 || q[2] >= E[2]) continue;
-    const long long b = B.bucket_base[D] + q[0] + (long long)E[0] * (q[1] + (long long)E[1] * q[2]);
-    total += __ldg(B.start + b + 1) - __ldg(B.start + b);
+    const int2 r = bucket_range(B, bucket_slot(B, D, E, q));
+    total += r.y - r.x;
   }
   return 2 * total;
 }
@@ -408,6 +494,7 @@ __device__ __forceinline__ int visit_bucket(int v) {
 }
 
 constexpr int kGatherThreads = 256;
+constexpr int kGatherBatch = 4;
 
 // One lane per listed face, a warp over 32 of them. A lane first loads the
 // ranges of its face's 8 distinct buckets (into shared memory, all at once),
@@ -424,8 +511,6 @@ __global__ void __launch_bounds__(kGatherThreads) k_splat_gather(int nx, int ny,
   const int *__restrict__ faces = B.sorted + B.face_off[D];
   const float4 *__restrict__ sposm = B.sposm;
   const float4 *__restrict__ svc = B.svc;
-  const int *__restrict__ start = B.start;
-  const long long base = B.bucket_base[D];
   const bool apic = B.apic;
   const double dx = X.dx;
   const int tid = threadIdx.x;
@@ -447,44 +532,54 @@ __global__ void __launch_bounds__(kGatherThreads) k_splat_gather(int nx, int ny,
       int q[3];
       bucket_coords<D>(k, fi, q);
       const bool out = !has || q[0] < 0 || q[0] >= E[0] || q[1] < 0 || q[1] >= E[1] || q[2] < 0 || q[2] >= E[2];
-      int2 r = make_int2(0, 0);
-      if (!out) {
-        const long long b = base + q[0] + (long long)E[0] * (q[1] + (long long)E[1] * q[2]);
-        r = make_int2(__ldg(start + b), __ldg(start + b + 1));
-      }
+      const int2 r = out ? make_int2(0, 0) : bucket_range(B, bucket_slot(B, D, E, q));
       range[k][tid] = r;
     }
     float m = 0.0f, mom = 0.0f;
     int v = -1, s = 0, e = 0;
     bool live = has;
     while (true) {
-      while (live && s == e) {
-        if (++v == 16) {
-          live = false;
-          break;
+      // the lane's next kGatherBatch particles of its visit sequence: their
+      // loads go out together so the L2 latencies overlap, and they are
+      // summed in sequence order
+      int at[kGatherBatch];
+      #pragma unroll
+      for (int u = 0; u < kGatherBatch; ++u) {
+        while (live && s == e) {
+          if (++v == 16) {
+            live = false;
+            break;
+          }
+          const int2 r = range[visit_bucket<D>(v)][tid];
+          s = r.x;
+          e = r.y;
         }
-        const int2 r = range[visit_bucket<D>(v)][tid];
-        s = r.x;
-        e = r.y;
+        at[u] = live ? s++ : -1;
       }
-      if (!__any_sync(0xffffffffu, live)) break;
-      if (live) {
-        const float4 pm = __ldg(sposm + s);
-        const float4 u = __ldg(svc + s);
-        ++s;
+      if (!__any_sync(0xffffffffu, at[0] >= 0)) break;
+      float4 pmb[kGatherBatch], ub[kGatherBatch];
+      #pragma unroll
+      for (int u = 0; u < kGatherBatch; ++u) {
+        pmb[u] = at[u] >= 0 ? __ldg(sposm + at[u]) : make_float4(0.f, 0.f, 0.f, 0.f);
+        ub[u] = at[u] >= 0 ? __ldg(svc + at[u]) : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+      #pragma unroll
+      for (int u = 0; u < kGatherBatch; ++u) {
+        if (at[u] < 0) continue;
+        const float4 pm = pmb[u], uv = ub[u];
         const float r0 = __double2float_rn((double)pm.x - pos[0]);
         const float r1 = __double2float_rn((double)pm.y - pos[1]);
         const float r2 = __double2float_rn((double)pm.z - pos[2]);
         const double w = tent<POW2>(r0, X) * tent<POW2>(r1, X) * tent<POW2>(r2, X);
         if (w != 0.0) {
           const double wm = w * (double)pm.w;
-          mom = __double2float_rn((double)mom + wm * (double)u.x);
+          mom = __double2float_rn((double)mom + wm * (double)uv.x);
           m = __double2float_rn((double)m + wm);
           if (apic) {
             double dot = 0.0;
-            dot += (double)u.y * (pos[0] - (double)pm.x);
-            dot += (double)u.z * (pos[1] - (double)pm.y);
-            dot += (double)u.w * (pos[2] - (double)pm.z);
+            dot += (double)uv.y * (pos[0] - (double)pm.x);
+            dot += (double)uv.z * (pos[1] - (double)pm.y);
+            dot += (double)uv.w * (pos[2] - (double)pm.z);
             mom = __double2float_rn((double)mom + wm * dot);
           }
         }
@@ -507,6 +602,21 @@ __global__ void __launch_bounds__(kGatherThreads) k_splat_gather(int nx, int ny,
       u[f] = __fdiv_rn(num, __fadd_rn(gm, m));
       ua[f] = 1;
     }
+  }
+}
+
+// The splat grid of axis D is zero and inactive wherever no particle
+// reaches; the gather writes only the faces the particles activate, so the
+// rest is cleared first (not after a refused bucket: then the call leaves
+// every grid as it was).
+template <int D>
+__global__ void k_splat_clear_grid(int nx, int ny, int nz, SplatBuffers B, SplatGrid G) {
+  if (B.nfaces[3]) return;
+  const size_t nf = (size_t)(nx + (D == 0)) * (ny + (D == 1)) * (nz + (D == 2));
+  for (size_t f = (size_t)blockIdx.x * blockDim.x + threadIdx.x; f < nf; f += (size_t)gridDim.x * blockDim.x) {
+    G.mass[D][f] = 0.0f;
+    G.momentum[D][f] = 0.0f;
+    G.splat_active[D][f] = 0;
   }
 }
 
@@ -537,6 +647,17 @@ void launch_exclusive_scan(int *data, long long n, int *tile_sums, cudaStream_t 
   k_scan_add<<<tiles, kScanThreads, 0, s>>>(data, n, tile_sums);
 }
 
+void launch_splat_bucket_scan(const SplatBuffers &B, int *tile_sums, cudaStream_t s) {
+  const unsigned blocks = (unsigned)((B.tiles + 1 + kTileWarps - 1) / kTileWarps);
+  k_splat_tile_scan<<<blocks, 32 * kTileWarps, 0, s>>>(B);
+  launch_exclusive_scan(B.tile_start, B.tiles + 1, tile_sums, s);
+}
+
+void launch_splat_clear(const SplatBuffers &B, cudaStream_t s) {
+  const unsigned blocks = (unsigned)((B.tiles + kTileWarps - 1) / kTileWarps);
+  if (blocks) k_splat_tile_clear<<<blocks, 32 * kTileWarps, 0, s>>>(B);
+}
+
 void launch_splat_scatter(long long count, const SplatBuffers &B, cudaStream_t s) {
   if (count <= 0) return;
   k_splat_scatter<<<(unsigned)((count + 255) / 256), 256, 0, s>>>(count, B);
@@ -564,6 +685,11 @@ void launch_splat_gather(int nx, int ny, int nz, double dx, const SplatBuffers &
   k_splat_face_sort<0><<<blocks, 256, 0, s>>>(B);
   k_splat_face_sort<1><<<blocks, 256, 0, s>>>(B);
   k_splat_face_sort<2><<<blocks, 256, 0, s>>>(B);
+  if (G.mass[0]) {
+    k_splat_clear_grid<0><<<blocks, 256, 0, s>>>(nx, ny, nz, B, G);
+    k_splat_clear_grid<1><<<blocks, 256, 0, s>>>(nx, ny, nz, B, G);
+    k_splat_clear_grid<2><<<blocks, 256, 0, s>>>(nx, ny, nz, B, G);
+  }
   const DxDiv X = make_dxdiv(dx);
   if (X.pow2) {
     k_splat_gather<0, true><<<blocks, kGatherThreads, 0, s>>>(nx, ny, nz, X, B, G);
