@@ -328,9 +328,9 @@ def run_splat(args):
                 "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_kind": peak_kind, "ms": call_ms, "algo_bytes_per_launch": algo, "traffic": traffic,
                 "note": ("not HBM-bound: the gather (about 3/5 of the call) is bound by FP64 issue and latency, "
-                         "each face summing its particles serially in the reference's order; traffic is 14x the "
-                         "algorithmic bytes because of the hash (bucket counters over the edge grids, packed and "
-                         "bucket-ordered particle copies)")}
+                         "each face summing its particles serially in the reference's order; traffic is 9.5x the "
+                         "algorithmic bytes because of the hash (packed and bucket-ordered particle copies, the "
+                         "gather's L2 re-reads)")}
     # end to end through the host-buffer entry point, pinned host arrays
     pin = lambda arr: torch.from_numpy(np.ascontiguousarray(arr)).pin_memory()
     h_rec = pin(P.view(np.uint8))
