@@ -84,10 +84,13 @@ typedef struct shkz_b200_config {
   int index_tile;             /* tile edge of the caller's grids (TileSize, default 16): unknown numbering of
                                  the warm-start vector */
   int spin_limit;             /* polling rounds of every bounded device wait (tile faces and flags of the MIC(0)
-                                 wavefronts) before it gives up and the call returns SHKZ_B200_ERR_TIMEOUT;
-                                 0 = the default, 2^21 (about 0.15 s) */
+                                 wavefronts, row values of shkz_b200_solve_csr's MIC(0) triangular solves) before
+                                 it gives up and the call returns SHKZ_B200_ERR_TIMEOUT; 0 = the default, 2^21
+                                 (about 0.15 s) for the wavefronts, 2^22 for the CSR solves */
   int fault_skip_publish;     /* fault injection, 0 = off: k > 0 makes the forward MIC(0) sweep's k-th wavefront
-                                 slot skip publishing its faces, so its consumers' bounded waits run out */
+                                 slot skip publishing its faces (and, in shkz_b200_solve_csr, the forward
+                                 triangular solve's k-th row in level order skip storing its value), so the
+                                 bounded waits on it run out */
   int device_mem_limit_mb;    /* cap on the device memory of the context's grid and tile-pool buffers, in MiB;
                                  a call that would exceed it returns SHKZ_B200_ERR_NOMEM (0 = no cap) */
   int csr_preconditioner;     /* shkz_b200_solve_csr: SHKZ_B200_PRECOND_NONE (default: what the shipped pcg

@@ -1449,13 +1449,20 @@ extern "C" int shkz_b200_apply_matrix(shkz_b200_ctx *ctx, const float *x_cells, 
 // x0 = 0 and the stopping rule ||r||inf <= Residual * ||b||inf.
 
 __global__ void k_csr_spmv64(int n, const int *__restrict__ indptr, const int *__restrict__ indices,
-                             const double *__restrict__ data, const double *__restrict__ x, double *__restrict__ y) {
+                             const double *__restrict__ data, const double *__restrict__ x, double *__restrict__ y,
+                             const CsrState *st) {
+  if (st->done) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     double s = 0.0;
     for (int p = indptr[i]; p < indptr[i + 1]; ++p) s += data[p] * x[indices[p]];
     y[i] = s;
   }
 }
+
+// Iterations of one CUDA graph launched between host checks of the CSR solve.
+// Every kernel returns at once after the stop, so launches past it cost only
+// their (empty) launch.
+constexpr int kCsrIterationsPerCheck = 16;
 
 extern "C" int shkz_b200_solve_csr(shkz_b200_ctx *ctx, long long n, const long long *indptr,
                                    const long long *indices, const double *data, const double *b, double *x,
@@ -1474,16 +1481,23 @@ extern "C" int shkz_b200_solve_csr(shkz_b200_ctx *ctx, long long n, const long l
   for (long long i = 0; i < nnz; ++i) hi[i] = (int)indices[i];
   int *dp = nullptr, *di = nullptr;
   double *dd = nullptr, *vb = nullptr;
+  CsrState *dst = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
   auto cleanup = [&]() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
     if (dp) cudaFree(dp);
     if (di) cudaFree(di);
     if (dd) cudaFree(dd);
     if (vb) cudaFree(vb);
+    if (dst) cudaFree(dst);
   };
   // vectors: r, x, s(p), z(q), the preconditioned residual and reduction scratch
   if (cudaMalloc(&dp, sizeof(int) * (n + 1)) != cudaSuccess || cudaMalloc(&di, sizeof(int) * (nnz ? nnz : 1)) != cudaSuccess ||
       cudaMalloc(&dd, sizeof(double) * (nnz ? nnz : 1)) != cudaSuccess ||
-      cudaMalloc(&vb, sizeof(double) * (5 * (size_t)n + 3 * 8192 + 8)) != cudaSuccess) {
+      cudaMalloc(&vb, sizeof(double) * (5 * (size_t)n + 3 * 8192 + 8)) != cudaSuccess ||
+      cudaMalloc(&dst, sizeof(CsrState)) != cudaSuccess) {
     cleanup();
     return res->status = SHKZ_B200_ERR_NOMEM;
   }
@@ -1496,6 +1510,8 @@ extern "C" int shkz_b200_solve_csr(shkz_b200_ctx *ctx, long long n, const long l
   cudaMemcpyAsync(r, b, sizeof(double) * n, cudaMemcpyHostToDevice, s);
   cudaMemsetAsync(xv, 0, sizeof(double) * n, s);
   CsrMic0 M;
+  if (ctx->cfg.spin_limit > 0) M.set_wait_limit(ctx->cfg.spin_limit);
+  if (ctx->cfg.fault_skip_publish > 0) M.set_fault_skip(ctx->cfg.fault_skip_publish - 1);
   if (mic) {
     int rc = M.build((int)n, hp.data(), hi.data(), dp, di, s);
     if (!rc) rc = M.factor(dd, ctx->cfg.mic_omega, ctx->cfg.mic_min_diag_ratio, s);
@@ -1504,53 +1520,78 @@ extern "C" int shkz_b200_solve_csr(shkz_b200_ctx *ctx, long long n, const long l
       return res->status = rc;
     }
   }
-  double h[3];
-  // out = {a.b, c.d, max|a|}
-  auto dots = [&](const double *a, const double *bb, const double *c, const double *d) -> bool {
-    launch_dots64((int)n, a, bb, c, d, part, cnt, out, s);
-    return cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, s) == cudaSuccess &&
-           cudaStreamSynchronize(s) == cudaSuccess;
-  };
   // z = M^-1 r (pcg_solver.h:378-385 with the MIC(0) result kept), or z = r
-  auto precondition = [&]() -> const double * {
-    if (!mic) return r;
-    M.apply(r, zv, s);
-    return zv;
-  };
-  int rc = 0, it = 0;
-  const double *z = precondition();
-  if (!dots(r, r, z, r)) { cleanup(); return res->status = SHKZ_B200_ERR_CUDA; }
+  const double *z = mic ? zv : r;
+  if (mic && M.apply(r, zv, s)) {
+    cleanup();
+    return res->status = SHKZ_B200_ERR_CUDA;
+  }
+  // out = {r.r, z.r, max|r|}
+  double h[3];
+  launch_dots64((int)n, r, r, z, r, part, cnt, out, s);
+  if (cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess) {
+    cleanup();
+    return res->status = SHKZ_B200_ERR_CUDA;
+  }
   const double r0 = h[2];
-  double rmax = r0;
-  if (r0 == 0.0) {
-    res->iterations = 0;
-    res->reresid = 0.0;
-  } else {
-    const double tol = ctx->cfg.residual * r0;
-    double rho = h[1];
+  int rc = 0;
+  res->iterations = 0;
+  res->reresid = r0 != 0.0 ? 1.0 : 0.0;
+  if (r0 != 0.0 && ctx->cfg.max_iterations > 0) {
+    // pcg_solver.h:252-295 on the device: q = A p, alpha = rho / p.q,
+    // x += alpha p, r -= alpha q, z = M^-1 r, stop on max|r| <= tol, else
+    // beta = z.r / rho, p = z + beta p
+    CsrState st{};
+    st.rho = h[1];
+    st.tol = ctx->cfg.residual * r0;
+    st.rmax = r0;
+    st.max_it = ctx->cfg.max_iterations;
+    cudaMemcpyAsync(dst, &st, sizeof(st), cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(p, z, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
     const int grid = (int)std::min<long long>((n + 255) / 256, 148 * 16);
-    for (it = 0; it < ctx->cfg.max_iterations; ++it) {
+    const long long counted = launches_so_far();
+    cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      k_csr_spmv64<<<grid, 256, 0, s>>>((int)n, dp, di, dd, p, q, dst);
       count_launches(1);
-      k_csr_spmv64<<<grid, 256, 0, s>>>((int)n, dp, di, dd, p, q);
-      if (!dots(p, q, nullptr, nullptr)) { rc = SHKZ_B200_ERR_CUDA; break; }
-      const double alpha = rho / h[0];
-      launch_axpy2_64((int)n, alpha, p, xv, q, r, s);
-      z = precondition();
-      if (!dots(r, r, z, r)) { rc = SHKZ_B200_ERR_CUDA; break; }
-      rmax = h[2];
-      if (!(rmax == rmax)) { rc = SHKZ_B200_ERR_NAN; break; }
-      if (rmax <= tol) { ++it; break; }
-      const double rho_new = h[1];
-      launch_xpby64((int)n, z, rho_new / rho, p, s);
-      rho = rho_new;
+      launch_csr_dots((int)n, p, q, nullptr, nullptr, part, cnt, dst, 0, s);
+      launch_csr_axpy2((int)n, dst, p, xv, q, r, s);
+      if (mic) M.apply(r, zv, s, &dst->done);
+      launch_csr_dots((int)n, r, r, z, r, part, cnt, dst, 1, s);
+      launch_csr_xpby((int)n, z, dst, p, s);
+      e = cudaStreamEndCapture(s, &graph);
     }
-    res->iterations = it;
-    res->reresid = rmax / r0;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+    // nodes of one iteration; counted again for every launch of the graph
+    const long long nodes = launches_so_far() - counted;
+    count_launches((int)-nodes);
+    while (e == cudaSuccess) {
+      for (int k = 0; k < kCsrIterationsPerCheck && e == cudaSuccess; ++k) {
+        e = cudaGraphLaunch(exec, s);
+        count_launches((int)nodes);
+      }
+      if (e == cudaSuccess) e = cudaMemcpyAsync(&st, dst, sizeof(st), cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      if (e != cudaSuccess || st.done) break;
+    }
+    if (e != cudaSuccess) {
+      shkz_set_cuda_error(e, "csr solve graph", __FILE__, __LINE__);
+      rc = SHKZ_B200_ERR_CUDA;
+    } else if (st.done == 3) {
+      rc = SHKZ_B200_ERR_NAN;
+    }
+    res->iterations = st.it;
+    res->reresid = st.rmax / r0;
   }
   if (cudaMemcpyAsync(x, xv, sizeof(double) * n, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
       cudaStreamSynchronize(s) != cudaSuccess)
     rc = SHKZ_B200_ERR_CUDA;
+  // a triangular solve's bounded wait that ran out outranks the NaN it left
+  if (mic && (!rc || rc == SHKZ_B200_ERR_NAN)) {
+    const int we = M.wait_error(s);
+    if (we) rc = we;
+  }
   cleanup();
   res->unknowns = n;
   res->outer_steps = mic ? M.levels() : 0;

@@ -1414,6 +1414,75 @@ __global__ void __launch_bounds__(256) k_axpy2_64(int n, double alpha, const dou
 __global__ void __launch_bounds__(256) k_xpby64(int n, const double *__restrict__ x, double beta, double *__restrict__ y) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = x[i] + beta * y[i];
 }
+// CSR loop on the device (CsrState): the reductions of k_dots64 in the same
+// order, with the scalar updates of the host loop in the last block
+__global__ void __launch_bounds__(256) k_csr_dots(int n, const double *__restrict__ a, const double *__restrict__ b,
+                                                  const double *__restrict__ c, const double *__restrict__ d,
+                                                  double *partials, unsigned *counter, CsrState *st, int phase) {
+  __shared__ double red[8];
+  if (st->done) return;
+  double s0 = 0.0, s1 = 0.0, m = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    s0 += a[i] * b[i];
+    if (c) s1 += c[i] * d[i];
+    m = fmax(m, fabs(a[i]));
+  }
+  s0 = block_sum<256>(s0, red);
+  s1 = block_sum<256>(s1, red);
+  m = block_max<256>(m, red);
+  if (threadIdx.x == 0) {
+    partials[3 * blockIdx.x] = s0;
+    partials[3 * blockIdx.x + 1] = s1;
+    partials[3 * blockIdx.x + 2] = m;
+  }
+  if (last_block(counter)) {
+    double t0 = 0, t1 = 0, tm = 0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += 256) {
+      t0 += partials[3 * i];
+      t1 += partials[3 * i + 1];
+      tm = fmax(tm, partials[3 * i + 2]);
+    }
+    t0 = block_sum<256>(t0, red);
+    t1 = block_sum<256>(t1, red);
+    tm = block_max<256>(tm, red);
+    if (threadIdx.x == 0) {
+      if (phase == 0) {
+        st->alpha = st->rho / t0;
+      } else {
+        // t1 = z.r, tm = max|r| (pcg_solver.h:262-281)
+        st->rmax = tm;
+        if (!(tm == tm)) {
+          st->done = 3;
+        } else if (tm <= st->tol) {
+          st->it += 1;
+          st->done = 1;
+        } else {
+          st->beta = t1 / st->rho;
+          st->rho = t1;
+          st->it += 1;
+          if (st->it >= st->max_it) st->done = 2;
+        }
+      }
+      *counter = 0;
+    }
+  }
+}
+__global__ void __launch_bounds__(256) k_csr_axpy2(int n, const CsrState *st, const double *__restrict__ x,
+                                                   double *__restrict__ y, const double *__restrict__ q,
+                                                   double *__restrict__ r) {
+  if (st->done) return;
+  const double alpha = st->alpha;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    y[i] += alpha * x[i];
+    r[i] -= alpha * q[i];
+  }
+}
+__global__ void __launch_bounds__(256) k_csr_xpby(int n, const double *__restrict__ x, const CsrState *st,
+                                                  double *__restrict__ y) {
+  if (st->done) return;
+  const double beta = st->beta;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = x[i] + beta * y[i];
+}
 // b32 = (float)(a64 * s)
 __global__ void __launch_bounds__(256) k_scale_f64_f32(int n, const double *__restrict__ a, double s, float *__restrict__ b) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = (float)(a[i] * s);
@@ -1714,6 +1783,20 @@ void launch_axpy2_64(int n, double alpha, const double *x, double *y, const doub
 void launch_xpby64(int n, const double *x, double beta, double *y, cudaStream_t s) {
   count_launches(1);
   k_xpby64<<<grid_for(n, 256 * 4, 148 * 8), 256, 0, s>>>(n, x, beta, y);
+}
+void launch_csr_dots(int n, const double *a, const double *b, const double *c, const double *d, double *partials,
+                     unsigned *counter, CsrState *st, int phase, cudaStream_t s) {
+  count_launches(1);
+  k_csr_dots<<<grid_for(n, 256 * 4, 148 * 8), 256, 0, s>>>(n, a, b, c, d, partials, counter, st, phase);
+}
+void launch_csr_axpy2(int n, const CsrState *st, const double *x, double *y, const double *q, double *r,
+                      cudaStream_t s) {
+  count_launches(1);
+  k_csr_axpy2<<<grid_for(n, 256 * 4, 148 * 8), 256, 0, s>>>(n, st, x, y, q, r);
+}
+void launch_csr_xpby(int n, const double *x, const CsrState *st, double *y, cudaStream_t s) {
+  count_launches(1);
+  k_csr_xpby<<<grid_for(n, 256 * 4, 148 * 8), 256, 0, s>>>(n, x, st, y);
 }
 void launch_scale_f64_f32(int n, const double *a, double sc, float *b, cudaStream_t s) {
   count_launches(1);

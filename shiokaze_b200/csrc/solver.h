@@ -53,6 +53,21 @@ void launch_dots64(int n, const double *a, const double *b, const double *c, con
                    unsigned *counter, double *out, cudaStream_t s);
 void launch_axpy2_64(int n, double alpha, const double *x, double *y, const double *q, double *r, cudaStream_t s);
 void launch_xpby64(int n, const double *x, double beta, double *y, cudaStream_t s);
+// The generic CSR solve's PCG loop kept on the device, so that one iteration
+// can be a CUDA graph launched many times between host checks. The kernels do
+// the arithmetic of k_dots64 / k_axpy2_64 / k_xpby64 with alpha and beta taken
+// from CsrState, and return at once when done != 0.
+struct CsrState {
+  double rho, alpha, beta, tol, rmax;
+  int it, done, status, max_it;  // done: 1 converged, 2 iteration limit, 3 NaN
+};
+// phase 0: alpha = rho / a.b; phase 1 (a = r, c = z, d = r): stop test on
+// max|r|, then rho, beta and the iteration count
+void launch_csr_dots(int n, const double *a, const double *b, const double *c, const double *d, double *partials,
+                     unsigned *counter, CsrState *st, int phase, cudaStream_t s);
+void launch_csr_axpy2(int n, const CsrState *st, const double *x, double *y, const double *q, double *r,
+                      cudaStream_t s);
+void launch_csr_xpby(int n, const double *x, const CsrState *st, double *y, cudaStream_t s);
 void launch_scale_f64_f32(int n, const double *a, double sc, float *b, cudaStream_t s);
 void launch_scale_f32_f64(int n, const float *a, double sc, double *b, cudaStream_t s);
 

@@ -10,6 +10,9 @@ failure as a status code instead, and the context stays usable:
   makes it run out on purpose: B200.FaultSkipPublish stops one tile of the
   forward MIC(0) sweep from publishing its faces (a flag that nothing sets),
   and B200.SpinLimit shortens the waits;
+* the same for the generic CSR solve's MIC(0) triangular solves: there
+  B200.FaultSkipPublish stops one row of the forward solve from storing its
+  value, and the rows that wait on it give up;
 * a device-memory cap that the tile pool does not fit under returns
   SHKZ_B200_ERR_NOMEM before cudaMalloc is asked;
 * a learned preconditioner that breaks down (a network of zeros) falls back to
@@ -59,6 +62,44 @@ def test_sweep_wait_timeout_returns_error_and_context_recovers():
     assert np.array_equal(p1, p0)
     for d in range(3):
         assert np.array_equal(v1[d], v0[d])
+
+
+def test_csr_solve_wait_timeout_returns_error_and_context_recovers():
+    import ctypes
+    from conftest import golden_names, load_golden
+    from shiokaze_b200 import native
+    g = load_golden(golden_names()[0])
+    n = int(g["rhs"].size)
+    indptr = np.ascontiguousarray(g["indptr"], np.int64)
+    indices = np.ascontiguousarray(g["indices"], np.int64)
+    data = np.ascontiguousarray(g["data"], np.float64)
+    b = np.ascontiguousarray(g["rhs"], np.float64)
+    L = native.load()
+
+    def solve(ctx):
+        x = np.zeros(n, np.float64)
+        res = native.Result()
+        rc = L.shkz_b200_solve_csr(ctx.handle, n, indptr.ctypes.data, indices.ctypes.data, data.ctypes.data,
+                                   b.ctypes.data, x.ctypes.data, ctypes.byref(res))
+        return rc, res, x
+
+    cfg = native.default_config()
+    cfg.residual = float(g["tol"])
+    cfg.csr_preconditioner = native.PRECOND_MIC0
+    rc0, res0, x0 = solve(native.Context(cfg))
+    assert rc0 == 0 and res0.iterations > 0
+    # the first row of the forward triangular solve never stores its value;
+    # the rows that depend on it give up after 20000 polling rounds
+    cfg.spin_limit, cfg.fault_skip_publish = 20000, 1
+    ctx = native.Context(cfg)
+    rc, _, _ = solve(ctx)
+    assert rc == ERR_TIMEOUT, rc
+    # the same context, fault off: the same solve as a fresh context's
+    cfg.spin_limit, cfg.fault_skip_publish = 0, 0
+    ctx.set_config(cfg)
+    rc1, res1, x1 = solve(ctx)
+    assert rc1 == 0 and res1.iterations == res0.iterations
+    assert np.array_equal(x1, x0)
 
 
 def test_device_memory_cap_returns_nomem_and_context_recovers():

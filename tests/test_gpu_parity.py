@@ -270,8 +270,9 @@ def test_solve_csr_matches_shipped_pcg(golden):
 
 def test_solve_csr_mic0_matches_reference_mic0(golden):
     """shkz_b200_solve_csr with csr_preconditioner = MIC0 on the reference's own
-    assembled CSR: the generic-matrix MIC(0) (factor and level-scheduled sweeps
-    on the device) against the reference's MIC(0)-PCG on the same system:
+    assembled CSR: the generic-matrix MIC(0) (level-scheduled factor and
+    sync-free triangular solves on the device) against the reference's
+    MIC(0)-PCG on the same system:
     iteration count within max(1, 2 %) and pressure within PARITY_TOL."""
     import ctypes
     from shiokaze_b200 import native
