@@ -199,32 +199,31 @@ __device__ __forceinline__ void stage_tile(const PoolSystem &S, const float *__r
     st4(pout + base, xv);
   }
   st4(&sm.xs[kk + 1][jj + 1][4 + 4 * q4], xv);
-  for (int h = tid; h < 384; h += 128) {
-    const int face = h >> 6, a = h & 63, u = a & 7, v = a >> 3;
-    const int nb = S.nbr[pt * 6 + face];
-    int cell;
-    switch (face) {
-      case NB_XM: cell = 7 + 8 * u + 64 * v; break;
-      case NB_XP: cell = 0 + 8 * u + 64 * v; break;
-      case NB_YM: cell = u + 8 * 7 + 64 * v; break;
-      case NB_YP: cell = u + 0 + 64 * v; break;
-      case NB_ZM: cell = u + 8 * v + 64 * 7; break;
-      default:    cell = u + 8 * v; break;
-    }
-    float val = 0.0f;
-    if (nb >= 0) {
-      const size_t o = (size_t)nb * SHKZ_TC + cell;
-      val = p[o];
-      if (zu) val = zu[o] + beta * val;
-    }
-    switch (face) {
-      case NB_XM: sm.xs[v + 1][u + 1][3] = val; break;
-      case NB_XP: sm.xs[v + 1][u + 1][12] = val; break;
-      case NB_YM: sm.xs[v + 1][0][u + 4] = val; break;
-      case NB_YP: sm.xs[v + 1][9][u + 4] = val; break;
-      case NB_ZM: sm.xs[0][v + 1][u + 4] = val; break;
-      default:    sm.xs[9][v + 1][u + 4] = val; break;
-    }
+  // The 6 x 64 halo values: three per thread, faces XM, YM, ZM for threads
+  // 0-63 and XP, YP, ZP for 64-127. Every load is issued before any is used,
+  // so the three neighbour lookups and the value loads each cost one round
+  // trip, not one per value.
+  const int a = tid & 63, u = a & 7, v = a >> 3, side = tid >> 6;
+  int nb[3];
+  #pragma unroll
+  for (int q = 0; q < 3; ++q) nb[q] = S.nbr[pt * 6 + 2 * q + side];
+  float hv[3], hz[3];
+  #pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    // cell of the neighbour tile next to this tile's face
+    const int cell = q == 0 ? (side ? 0 : 7) + 8 * u + 64 * v
+                   : q == 1 ? u + (side ? 0 : 56) + 64 * v
+                            : u + 8 * v + (side ? 0 : 448);
+    const size_t o = (size_t)(nb[q] >= 0 ? nb[q] : 0) * SHKZ_TC + cell;
+    hv[q] = nb[q] >= 0 ? p[o] : 0.0f;
+    hz[q] = (zu && nb[q] >= 0) ? zu[o] : 0.0f;
+  }
+  #pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    const float val = (zu && nb[q] >= 0) ? hz[q] + beta * hv[q] : hv[q];
+    if (q == 0) sm.xs[v + 1][u + 1][side ? 12 : 3] = val;
+    else if (q == 1) sm.xs[v + 1][side ? 9 : 0][u + 4] = val;
+    else sm.xs[side ? 9 : 0][v + 1][u + 4] = val;
   }
 }
 
