@@ -407,9 +407,9 @@ extern "C" void shkz_b200_destroy(shkz_b200_ctx *ctx) {
                   ctx->h_vact[0], ctx->h_vact[1], ctx->h_vact[2], ctx->h_pact, ctx->flags, ctx->unk, ctx->tile_count,
                   ctx->tile_state, ctx->pool_tile, ctx->nbr, ctx->level_count, ctx->sched, ctx->bsum, ctx->total,
                   ctx->diag, ctx->offx, ctx->offy, ctx->offz, ctx->d32, ctx->diag64, ctx->offx64, ctx->offy64,
-                  ctx->offz64, ctx->rhs64, ctx->upx, ctx->upy, ctx->upz, ctx->colsum, ctx->dmic64, ctx->x64, ctx->r64, ctx->xref64, ctx->p64, ctx->q64,
-                  ctx->z64, ctx->x, ctx->r,
-                  ctx->p, ctx->q, ctx->z, ctx->t, ctx->p32, ctx->partials, ctx->out4, ctx->counter, ctx->st,
+                  ctx->offz64, ctx->rhs64, ctx->upx, ctx->upy, ctx->upz, ctx->colsum, ctx->dmic64, ctx->x64,
+                  ctx->r64, ctx->xref64, ctx->p64, ctx->q64, ctx->z64, ctx->x, ctx->r, ctx->p, ctx->q, ctx->z,
+                  ctx->t, ctx->p32, ctx->partials, ctx->out4, ctx->counter, ctx->st,
                   ctx->wflags, ctx->faces_f, ctx->faces_b, ctx->ws, ctx->st_scratch, ctx->mcount, ctx->mstate,
                   ctx->mtile, ctx->mnbr, ctx->msched, ctx->msub, ctx->mfaces_f, ctx->mfaces_b, ctx->curv,
                   ctx->prev, ctx->rank_pool, ctx->rank_cnt, ctx->rank_total, ctx->xw, ctx->h_dens[0],
@@ -417,8 +417,9 @@ extern "C" void shkz_b200_destroy(shkz_b200_ctx *ctx) {
                   ctx->ext_a[0], ctx->ext_a[1], ctx->ext_a[2], ctx->ext_flag, ctx->sp_raw, ctx->sp_posm,
                   ctx->sp_vc[0], ctx->sp_vc[1], ctx->sp_vc[2], ctx->sp_key, ctx->sp_rank, ctx->sp_list, ctx->sp_sposm,
                   ctx->sp_svc, ctx->sp_faces, ctx->sp_sorted, ctx->sp_face_bin, ctx->sp_nfaces, ctx->sp_work,
-                  ctx->sp_count, ctx->sp_tile_start, ctx->sp_tile_act, ctx->sp_tiles, ctx->sp_act[0], ctx->sp_act[1], ctx->sp_act[2], ctx->sp_mass[0],
-                  ctx->sp_mass[1], ctx->sp_mass[2], ctx->sp_mom[0], ctx->sp_mom[1], ctx->sp_mom[2],
+                  ctx->sp_count, ctx->sp_tile_start, ctx->sp_tile_act, ctx->sp_tiles, ctx->sp_act[0],
+                  ctx->sp_act[1], ctx->sp_act[2], ctx->sp_mass[0], ctx->sp_mass[1], ctx->sp_mass[2], ctx->sp_mom[0],
+                  ctx->sp_mom[1], ctx->sp_mom[2],
                   ctx->sp_sact[0], ctx->sp_sact[1], ctx->sp_sact[2]};
   for (void *p : ptrs)
     if (p) cudaFree(p);
