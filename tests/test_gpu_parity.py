@@ -429,3 +429,32 @@ def test_solve_csr_edge_cases(pre):
     # summation order alone moves long unpreconditioned CG runs by a few percent
     assert abs(res.iterations - it_o) <= max(1, int((0.02 if pre else 0.05) * it_o)), (res.iterations, it_o)
     assert np.abs(x - xo[:n]).max() <= 1e-6 * np.abs(xo).max()
+
+
+def test_one_context_across_scenes_matches_fresh_contexts():
+    """A projection module lives through a simulation whose grid can change
+    (a new scene, a resized domain): one context runs scenes of five shapes in
+    turn, some twice, growing and shrinking its tile pool, macro tiles and
+    wavefront buffers, and every projection is bit-identical (pressure,
+    velocities, masks, iteration count) to the same projection on a fresh
+    context."""
+    from shiokaze_b200 import scenes
+    from shiokaze_b200.projection import grids_from_scene
+    seq = [scenes.dambreak_sphere(n=48, seed=2, tol=1e-6), scenes.sloshing_tank(n=96, seed=1, tol=1e-6),
+           scenes.splash(n=80, seed=4, tol=1e-6, spheres=30), scenes.dambreak_sphere(n=48, seed=2, tol=1e-6),
+           scenes.training_scene(n=64, seed=3), scenes.sloshing_tank(n=96, seed=1, tol=1e-6),
+           scenes.dambreak_sphere(n=20, seed=5, tol=1e-6)]
+    shared = solver(Residual=1e-6)
+    for sc in seq:
+        shared.initialize((sc.nx, sc.ny, sc.nz), sc.dx)
+        vel, solid, svel, fluid = grids_from_scene(sc)
+        res = shared.project(sc.dt, vel, solid, svel, fluid)
+        fresh, res0, vel0 = run(sc, Residual=1e-6)
+        assert res["status"] == 0 and res0["status"] == 0, (res, res0)
+        assert res["iterations"] == res0["iterations"], (sc.name, sc.nx, res["iterations"], res0["iterations"])
+        p, p0 = shared.get_pressure(), fresh.get_pressure()
+        assert np.array_equal(p.active, p0.active)
+        assert np.array_equal(p.values.view(np.uint32), p0.values.view(np.uint32)), (sc.name, sc.nx)
+        for d in range(3):
+            assert np.array_equal(vel.active[d], vel0.active[d])
+            assert np.array_equal(vel.values[d].view(np.uint32), vel0.values[d].view(np.uint32)), (sc.name, d)
